@@ -1,0 +1,174 @@
+/*
+ * lfts_b200 -- C ABI of the B200 (sm_100a) Langevin field-theoretic simulation
+ * step for AB diblock copolymers.
+ *
+ * The entry points replace the C++ methods the reference driver calls
+ * (tmbeardsley/lfts_cpu); each declaration cites the method it stands in for.
+ * All state lives on one GPU inside an opaque context; host pointers are plain
+ * C arrays with the reference's layouts:
+ *   fields   w = [W-(M) | w+(M) | phi-(M) | phi+(M)]       (src/lfts_simulation.h:21)
+ *   mesh     r = mz*(i*my + j) + k                         (src/field_generator.h:18)
+ *   spectrum k = k2 + (mz/2+1)*(K1 + my*K0), Mk entries    (src/step.cc:83)
+ * Every call returns an lfts_status (0 = success).  A context is used by one
+ * host thread at a time.  Calls are synchronous unless the name ends in _async.
+ * There is no CPU fallback: a missing GPU or unsupported mesh is an error.
+ */
+#ifndef LFTS_B200_H
+#define LFTS_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum lfts_status {
+    LFTS_OK = 0,
+    LFTS_ERR_ARG = 1,          /* bad argument (null pointer, size, index) */
+    LFTS_ERR_UNSUPPORTED = 2,  /* mesh size without an FFT kernel, or odd my */
+    LFTS_ERR_CUDA = 3,         /* CUDA runtime error (see lfts_last_error_string) */
+    LFTS_ERR_NOMEM = 4,        /* device allocation failed */
+    LFTS_ERR_SINGULAR = 5,     /* Anderson least-squares matrix singular */
+    LFTS_ERR_STATE = 6,        /* call out of order (e.g. fields never set) */
+    LFTS_ERR_NOTCONV = 7       /* reserved: iteration cap reached where one is fatal */
+} lfts_status;
+
+typedef enum lfts_precision {
+    LFTS_FP64 = 0,       /* everything FP64: matches the reference to ~1e-10 */
+    LFTS_FP32_MIXED = 1  /* FP32 FFTs/propagators; FP64 Q, log, Anderson, H, fields */
+} lfts_precision;
+
+/* Simulation constants after the reference's input conversion
+ * (src/lfts_params.cc:87-119): XbN is the bare chi*N actually simulated. */
+typedef struct lfts_params {
+    int N;         /* monomers per chain */
+    int NA;        /* A-block length (NB = N - NA) */
+    double XbN;    /* bare chi * N */
+    double C;      /* sqrt(Nbar) */
+    double dt;     /* Langevin time step * N */
+    int m[3];      /* mesh mx, my, mz */
+    double L[3];   /* box Lx, Ly, Lz in R0 */
+} lfts_params;
+
+typedef struct lfts_ctx lfts_ctx;
+
+const char *lfts_version(void);
+const char *lfts_status_string(int status);
+/* text of the last CUDA error seen by any call in this process */
+const char *lfts_last_error_string(void);
+/* 1 when mesh dimension n has an FFT kernel in this build */
+int lfts_mesh_supported(int n);
+
+/* Allocates device state for one system: the diblock, step, anderson and
+ * strFunc objects of lfts_simulation's constructor (src/lfts_simulation.cc:29-42). */
+int lfts_create(const lfts_params *p, int precision, int device, lfts_ctx **out);
+int lfts_destroy(lfts_ctx *ctx);
+/* device bytes held by the context */
+int lfts_device_bytes(const lfts_ctx *ctx, size_t *bytes);
+
+/* Upload W- and w+ (2M doubles, host); replaces the reference's readArray /
+ * generate_field into w_ (src/lfts_simulation.cc:45-49). */
+int lfts_set_fields(lfts_ctx *ctx, const double *w_host);
+/* Download w = [W-, w+, phi-, phi+] (4M doubles, host). */
+int lfts_get_fields(lfts_ctx *ctx, double *w_host);
+/* Device address of the FP64 field array (4M doubles) owned by the context. */
+int lfts_fields_device(lfts_ctx *ctx, double **w_dev);
+
+/* diblock::calc_concs (src/diblock.cc:30-60): phi-, phi+ from W-, w+; ln Q out. */
+int lfts_calc_concs(lfts_ctx *ctx, double *lnQ);
+
+/* anderson::mix (src/anderson.cc:24-93): saddle point of w+ by Anderson
+ * mixing with history 10; *k_out receives the reference's return value. */
+int lfts_anderson_mix(lfts_ctx *ctx, int maxIter, double errTol, int *k_out);
+
+/* langevin::langevin (src/langevin.cc:7-17): the initial "previous" noise, M
+ * doubles already scaled by sigma, drawn by the caller's generator. */
+int lfts_langevin_init(lfts_ctx *ctx, const double *noise_prev_host);
+/* langevin::step_wm (src/langevin.cc:23-37): W- += -(phi- + 2W-/XbN) dt +
+ * (eta_prev + eta_new)/2 with the caller's new noise (M doubles, host). */
+int lfts_langevin_step(lfts_ctx *ctx, const double *noise_new_host);
+/* same with the new noise already in device memory */
+int lfts_langevin_step_device(lfts_ctx *ctx, const double *noise_new_dev);
+
+/* One reference Langevin step (src/lfts_simulation.cc:69-76): step_wm, mix,
+ * then the extra calc_concs whose ln Q the reference prints. */
+int lfts_langevin_full_step(lfts_ctx *ctx, const double *noise_new_dev, int maxIter,
+                            double errTol, int *k_out, double *lnQ);
+
+/* strFunc::sample (src/strFunc.cc:36-46): S(k) += |FFT(W-)(k)|^2 */
+int lfts_sk_sample(lfts_ctx *ctx);
+/* raw accumulator (Mk doubles) and the number of samples */
+int lfts_sk_get(lfts_ctx *ctx, double *S_host, int *nsamples);
+int lfts_sk_reset(lfts_ctx *ctx);
+/* strFunc::save averaging (src/strFunc.cc:50-76): spherical average over |K|
+ * with tolerance dK.  K_out and S_out hold at least Mk entries; *nbins out. */
+int lfts_sk_bin(lfts_ctx *ctx, double dK, double *K_out, double *S_out, int *nbins);
+
+/* lfts_simulation::getH (src/lfts_simulation.cc:122-135) */
+int lfts_get_H(lfts_ctx *ctx, double *H);
+
+/* step::fwd (src/step.cc:35-65): one contour step of both chains.
+ * q_in, q_out, h: 2M doubles each (host); i: monomer index of q_in. */
+int lfts_step_fwd(lfts_ctx *ctx, const double *q_in, double *q_out, const double *h, int i);
+/* step::update_g_lookup (src/step.cc:69-89): the Mk Boltzmann weights g(k) */
+int lfts_g_lookup(lfts_ctx *ctx, double *g_host);
+
+/* ---- timing / integration helpers -------------------------------------- */
+/* The CUDA stream every call of this context runs on (a cudaStream_t). */
+void *lfts_stream(lfts_ctx *ctx);
+/* Run the contour chain of one calc_concs with CUDA events around every
+ * launch: mean ms of a yz-plane step kernel, of an x-pencil kernel, and the
+ * whole chain (leaves the propagators of the current fields). */
+int lfts_profile_chain(lfts_ctx *ctx, double *ms_plane, double *ms_pencil, double *ms_chain);
+/* Number of kernels this context has launched so far. */
+long long lfts_kernel_launches(const lfts_ctx *ctx);
+/* Mean Anderson iteration count of all lfts_anderson_mix calls so far. */
+int lfts_anderson_stats(const lfts_ctx *ctx, long long *calls, long long *iterations);
+/* Copy the propagators of the last calc_concs, 2(N+1)M doubles (slot 0
+ * zero), layout of src/diblock.cc:19-24. */
+int lfts_get_propagators(lfts_ctx *ctx, double *q_host);
+
+
+/* ---- host helpers with the reference driver's semantics ------------------ */
+/* Everything the reference's lfts_params derives from the 3-line input header
+ * (src/lfts_params.cc:87-119). */
+typedef struct lfts_input {
+    int N, NA, NB;
+    double XN_in;      /* XN as written in the file */
+    double C, dt;
+    int isXeN;
+    int m[3];
+    double L[3];
+    int equil_its, sim_its, sample_freq, save_freq, loadType;
+    /* derived */
+    double XbN, XeN, V, sigma;
+    long long M, Mk;
+} lfts_input;
+
+/* lfts_params::read_Input_Params + calculate_Derived_Params: step counts
+ * rounded down to multiples of sample_freq, chi converted through z_inf. */
+int lfts_read_input(const char *path, lfts_input *out);
+/* lfts_params::z_inf_discrete (src/lfts_params.cc:122-142) */
+double lfts_z_inf_discrete(const double L[3], const int m[3], int N, double Nbar, int tmax);
+/* Fill the simulation constants from a parsed input. */
+void lfts_params_from_input(const lfts_input *in, lfts_params *p);
+
+/* The reference's generator: std::mt19937_64 seeded with `seed` feeding ONE
+ * std::normal_distribution(0, sigma) (it keeps a cached spare deviate) and
+ * uniform_real_distribution(0, 1) draws (src/langevin.cc:13-16,28;
+ * src/lfts_simulation.cc:23,149-155).  Same libstdc++ => same stream. */
+typedef struct lfts_rng lfts_rng;
+int lfts_rng_create(unsigned long long seed, double sigma, lfts_rng **out);
+int lfts_rng_destroy(lfts_rng *r);
+int lfts_rng_normal(lfts_rng *r, long long n, double *out);
+int lfts_rng_uniform(lfts_rng *r, long long n, double *out);
+/* field_generator::create_lamellar (src/field_generator.h:11-24), W- and w+ */
+int lfts_lamellar_field(double *w, double amplitude, const int m[3], int kx, int ky, int kz);
+/* lfts_simulation::generate_field default branch (src/lfts_simulation.cc:149-155):
+ * W- = XbN (U(0,1) - 1/2), w+ = 0, drawing M uniforms from r. */
+int lfts_random_field(lfts_rng *r, double *w, double XbN, long long M);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

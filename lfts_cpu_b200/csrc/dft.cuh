@@ -1,0 +1,206 @@
+// Complex arithmetic and in-register small DFTs for the sm_100a FFT kernels.
+//
+// Convention (the one FFTW documents and the reference relies on at
+// src/step.cc:41,50): forward X[k] = sum_j x[j] exp(-2 pi i jk/n), backward
+// with +i, both unnormalised.  S = -1 selects forward, S = +1 backward.
+//
+// Radices 2, 3, 4, 5 are written out; 6, 8, 10, 12, 16 are two-level
+// Cooley-Tukey compositions of those with compile-time twiddles.  All
+// constants are exact values of cos/sin at multiples of 1.5 degrees
+// (the finest angle any supported radix needs), given to 20 digits.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace lfts {
+
+template <typename T>
+struct alignas(2 * sizeof(T)) cpx {
+    T x, y;
+};
+
+template <typename T>
+__device__ __forceinline__ cpx<T> cadd(cpx<T> a, cpx<T> b) { return {a.x + b.x, a.y + b.y}; }
+template <typename T>
+__device__ __forceinline__ cpx<T> csub(cpx<T> a, cpx<T> b) { return {a.x - b.x, a.y - b.y}; }
+template <typename T>
+__device__ __forceinline__ cpx<T> cmul(cpx<T> a, cpx<T> b)
+{
+    return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+// a * conj(b)
+template <typename T>
+__device__ __forceinline__ cpx<T> cmulc(cpx<T> a, cpx<T> b)
+{
+    return {a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y};
+}
+template <typename T>
+__device__ __forceinline__ cpx<T> cscale(cpx<T> a, T s) { return {a.x * s, a.y * s}; }
+// a * (S i)
+template <int S, typename T>
+__device__ __forceinline__ cpx<T> cmul_i(cpx<T> a)
+{
+    return S > 0 ? cpx<T>{-a.y, a.x} : cpx<T>{a.y, -a.x};
+}
+// a times the table twiddle tw = exp(-2 pi i t/n) (forward) or its conjugate (backward)
+template <int S, typename T>
+__device__ __forceinline__ cpx<T> ctw(cpx<T> a, cpx<T> tw)
+{
+    return S < 0 ? cmul(a, tw) : cmulc(a, tw);
+}
+
+// cos and sin of 2 pi e / R for R dividing 240 (1.5-degree units).
+__host__ __device__ constexpr double root_cos_sin(int e, int R, bool want_sin)
+{
+    int t = ((e % R + R) % R) * (240 / R);
+    int q = t / 60, rem = t % 60;
+    double c = 1.0, s = 0.0;
+    switch (rem) {
+        case 0: c = 1.0; s = 0.0; break;
+        case 12: c = 0.95105651629515357212; s = 0.30901699437494742410; break;
+        case 15: c = 0.92387953251128675613; s = 0.38268343236508977173; break;
+        case 20: c = 0.86602540378443864676; s = 0.5; break;
+        case 24: c = 0.80901699437494742410; s = 0.58778525229247312917; break;
+        case 30: c = 0.70710678118654752440; s = 0.70710678118654752440; break;
+        case 36: c = 0.58778525229247312917; s = 0.80901699437494742410; break;
+        case 40: c = 0.5; s = 0.86602540378443864676; break;
+        case 45: c = 0.38268343236508977173; s = 0.92387953251128675613; break;
+        case 48: c = 0.30901699437494742410; s = 0.95105651629515357212; break;
+        default: c = 0.0; s = 0.0; break;  // unreachable for supported radices
+    }
+    double cq = q == 0 ? c : q == 1 ? -s : q == 2 ? -c : s;
+    double sq = q == 0 ? s : q == 1 ? c : q == 2 ? -s : -c;
+    return want_sin ? sq : cq;
+}
+
+// a * exp(S 2 pi i e / R), e and R compile-time after unrolling
+template <int S, int R, typename T>
+__device__ __forceinline__ cpx<T> croot(cpx<T> a, int e)
+{
+    const int t = ((e % R) + R) % R;
+    if (t == 0) return a;
+    if (4 * t == R) return cmul_i<S>(a);
+    if (2 * t == R) return {-a.x, -a.y};
+    if (4 * t == 3 * R) return cmul_i<-S>(a);
+    const T c = (T)root_cos_sin(t, R, false);
+    const T s = (T)(S * root_cos_sin(t, R, true));
+    return {a.x * c - a.y * s, a.x * s + a.y * c};
+}
+
+template <int R>
+struct Split;  // R = A * B used by the composite DFT
+template <> struct Split<6> { static constexpr int A = 3, B = 2; };
+template <> struct Split<8> { static constexpr int A = 4, B = 2; };
+template <> struct Split<10> { static constexpr int A = 5, B = 2; };
+template <> struct Split<12> { static constexpr int A = 4, B = 3; };
+template <> struct Split<16> { static constexpr int A = 4, B = 4; };
+
+template <int R, int S, typename T>
+struct Dft {
+    // X[ka + A kb] = sum_jb w_B^{jb kb} w_R^{jb ka} sum_ja x[jb + B ja] w_A^{ja ka}
+    static __device__ __forceinline__ void run(cpx<T> *v)
+    {
+        constexpr int A = Split<R>::A, B = Split<R>::B;
+        cpx<T> y[R];
+#pragma unroll
+        for (int jb = 0; jb < B; jb++) {
+            cpx<T> t[A];
+#pragma unroll
+            for (int ja = 0; ja < A; ja++) t[ja] = v[jb + B * ja];
+            Dft<A, S, T>::run(t);
+#pragma unroll
+            for (int ka = 0; ka < A; ka++) y[jb * A + ka] = croot<S, R>(t[ka], jb * ka);
+        }
+#pragma unroll
+        for (int ka = 0; ka < A; ka++) {
+            cpx<T> u[B];
+#pragma unroll
+            for (int jb = 0; jb < B; jb++) u[jb] = y[jb * A + ka];
+            Dft<B, S, T>::run(u);
+#pragma unroll
+            for (int kb = 0; kb < B; kb++) v[ka + A * kb] = u[kb];
+        }
+    }
+};
+
+template <int S, typename T>
+struct Dft<1, S, T> {
+    static __device__ __forceinline__ void run(cpx<T> *) {}
+};
+
+template <int S, typename T>
+struct Dft<2, S, T> {
+    static __device__ __forceinline__ void run(cpx<T> *v)
+    {
+        cpx<T> a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    }
+};
+
+template <int S, typename T>
+struct Dft<3, S, T> {
+    static __device__ __forceinline__ void run(cpx<T> *v)
+    {
+        const T h = (T)0.86602540378443864676;  // sin(2 pi / 3)
+        cpx<T> s = cadd(v[1], v[2]), d = csub(v[1], v[2]);
+        cpx<T> m = {v[0].x - (T)0.5 * s.x, v[0].y - (T)0.5 * s.y};
+        cpx<T> r = cmul_i<S>(cscale(d, h));
+        v[0] = cadd(v[0], s);
+        v[1] = cadd(m, r);
+        v[2] = csub(m, r);
+    }
+};
+
+template <int S, typename T>
+struct Dft<4, S, T> {
+    static __device__ __forceinline__ void run(cpx<T> *v)
+    {
+        cpx<T> a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+        cpx<T> b0 = cadd(v[1], v[3]), b1 = cmul_i<S>(csub(v[1], v[3]));
+        v[0] = cadd(a0, b0);
+        v[2] = csub(a0, b0);
+        v[1] = cadd(a1, b1);
+        v[3] = csub(a1, b1);
+    }
+};
+
+template <int S, typename T>
+struct Dft<5, S, T> {
+    static __device__ __forceinline__ void run(cpx<T> *v)
+    {
+        const T c1 = (T)0.30901699437494742410;   // cos(2 pi/5)
+        const T c2 = (T)-0.80901699437494742410;  // cos(4 pi/5)
+        const T s1 = (T)0.95105651629515357212;   // sin(2 pi/5)
+        const T s2 = (T)0.58778525229247312917;   // sin(4 pi/5)
+        cpx<T> b1 = cadd(v[1], v[4]), b2 = cadd(v[2], v[3]);
+        cpx<T> d1 = csub(v[1], v[4]), d2 = csub(v[2], v[3]);
+        cpx<T> x0 = v[0];
+        cpx<T> p1 = {x0.x + c1 * b1.x + c2 * b2.x, x0.y + c1 * b1.y + c2 * b2.y};
+        cpx<T> p2 = {x0.x + c2 * b1.x + c1 * b2.x, x0.y + c2 * b1.y + c1 * b2.y};
+        cpx<T> q1 = cmul_i<S>(cpx<T>{s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y});
+        cpx<T> q2 = cmul_i<S>(cpx<T>{s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y});
+        v[0] = cadd(x0, cadd(b1, b2));
+        v[1] = cadd(p1, q1);
+        v[4] = csub(p1, q1);
+        v[2] = cadd(p2, q2);
+        v[3] = csub(p2, q2);
+    }
+};
+
+// Two-stage plan of a supported line length n = R1 * R2.
+template <int N>
+struct Plan;
+template <> struct Plan<8> { static constexpr int R1 = 4, R2 = 2; };
+template <> struct Plan<12> { static constexpr int R1 = 4, R2 = 3; };
+template <> struct Plan<16> { static constexpr int R1 = 4, R2 = 4; };
+template <> struct Plan<20> { static constexpr int R1 = 5, R2 = 4; };
+template <> struct Plan<24> { static constexpr int R1 = 8, R2 = 3; };
+template <> struct Plan<32> { static constexpr int R1 = 8, R2 = 4; };
+template <> struct Plan<40> { static constexpr int R1 = 8, R2 = 5; };
+template <> struct Plan<48> { static constexpr int R1 = 8, R2 = 6; };
+template <> struct Plan<64> { static constexpr int R1 = 8, R2 = 8; };
+template <> struct Plan<80> { static constexpr int R1 = 16, R2 = 5; };
+template <> struct Plan<96> { static constexpr int R1 = 12, R2 = 8; };
+template <> struct Plan<128> { static constexpr int R1 = 16, R2 = 8; };
+
+}  // namespace lfts

@@ -1,0 +1,35 @@
+// Lookup of the compiled FFT kernels by mesh size (one translation unit per
+// precision instantiates them: fft_fp64.cu, fft_fp32.cu).
+#pragma once
+#include <cstddef>
+
+#include "fft_kernels.cuh"
+
+namespace lfts {
+
+template <typename T>
+struct PlaneKernels {
+    void (*fn[4])(PlaneArgs<T>);  // indexed by PlaneMode
+    int nt;
+    size_t smem;
+};
+
+template <typename T>
+struct PencilKernels {
+    void (*fn[2])(PencilArgs<T>);  // indexed by PencilMode
+    int nt;
+    size_t smem;
+    int cw;
+};
+
+// false when (ny, nz) / nx has no instantiation in this build
+bool plane_kernels(int ny, int nz, PlaneKernels<double> *out);
+bool plane_kernels(int ny, int nz, PlaneKernels<float> *out);
+bool pencil_kernels(int nx, PencilKernels<double> *out);
+bool pencil_kernels(int nx, PencilKernels<float> *out);
+// line lengths with a two-stage plan
+bool fft_length_supported(int n);
+// (ny, nz) plane pairs with an instantiation
+bool plane_pair_supported(int ny, int nz);
+
+}  // namespace lfts

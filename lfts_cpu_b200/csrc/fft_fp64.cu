@@ -1,0 +1,25 @@
+// FP64 instantiations of the contour-step FFT kernels.
+#include "fft_inst.cuh"
+
+#define LFTS_PLANE_CASE_double(a, b) \
+    if (ny == a && nz == b) { fill_plane<double, a, b>(o); return true; }
+#define LFTS_PENCIL_CASE_double(a) \
+    if (nx == a) { fill_pencil<double, a>(o); return true; }
+LFTS_DEFINE_DISPATCH(double)
+
+namespace lfts {
+bool fft_length_supported(int n)
+{
+#define LFTS_LEN_CASE(a) if (n == a) return true;
+    LFTS_FOR_EACH_LEN(LFTS_LEN_CASE)
+#undef LFTS_LEN_CASE
+    return false;
+}
+bool plane_pair_supported(int ny, int nz)
+{
+#define LFTS_PAIR_CASE(a, b) if (ny == a && nz == b) return true;
+    LFTS_FOR_EACH_PAIR(LFTS_PAIR_CASE)
+#undef LFTS_PAIR_CASE
+    return false;
+}
+}  // namespace lfts

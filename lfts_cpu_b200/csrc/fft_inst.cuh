@@ -1,0 +1,52 @@
+// Instantiation lists of the FFT kernels, shared by fft_fp64.cu / fft_fp32.cu.
+#pragma once
+#include "fft_dispatch.h"
+
+// line lengths (each needs a Plan<> in dft.cuh)
+#define LFTS_FOR_EACH_LEN(X) X(8) X(12) X(16) X(20) X(24) X(32) X(40) X(48) X(64) X(80) X(96) X(128)
+// (ny, nz) plane pairs: the cubic ones plus a few boxes used by tests
+#define LFTS_FOR_EACH_PAIR(X)                                                                  \
+    X(8, 8) X(12, 12) X(16, 16) X(20, 20) X(24, 24) X(32, 32) X(40, 40) X(48, 48) X(64, 64)   \
+    X(80, 80) X(96, 96) X(128, 128) X(12, 20) X(24, 16) X(16, 32) X(32, 64)
+
+namespace lfts {
+
+template <typename T, int NY, int NZ>
+static void fill_plane(PlaneKernels<T> *o)
+{
+    using C = PlaneCfg<T, NY, NZ>;
+    o->fn[PLANE_INIT_W] = plane_kernel<T, NY, NZ, PLANE_INIT_W>;
+    o->fn[PLANE_INIT_Q] = plane_kernel<T, NY, NZ, PLANE_INIT_Q>;
+    o->fn[PLANE_STEP] = plane_kernel<T, NY, NZ, PLANE_STEP>;
+    o->fn[PLANE_LAST] = plane_kernel<T, NY, NZ, PLANE_LAST>;
+    o->nt = C::NT;
+    o->smem = C::SMEM;
+}
+
+template <typename T, int NX>
+static void fill_pencil(PencilKernels<T> *o)
+{
+    constexpr int CW = 32;
+    using C = PencilCfg<T, NX, CW>;
+    o->fn[PENCIL_CONV] = pencil_kernel<T, NX, CW, PENCIL_CONV>;
+    o->fn[PENCIL_POWER] = pencil_kernel<T, NX, CW, PENCIL_POWER>;
+    o->nt = C::NT;
+    o->smem = C::SMEM;
+    o->cw = CW;
+}
+
+}  // namespace lfts
+
+#define LFTS_DEFINE_DISPATCH(T)                                                       \
+    namespace lfts {                                                                  \
+    bool plane_kernels(int ny, int nz, PlaneKernels<T> *o)                            \
+    {                                                                                 \
+        LFTS_FOR_EACH_PAIR(LFTS_PLANE_CASE_##T)                                       \
+        return false;                                                                 \
+    }                                                                                 \
+    bool pencil_kernels(int nx, PencilKernels<T> *o)                                  \
+    {                                                                                 \
+        LFTS_FOR_EACH_LEN(LFTS_PENCIL_CASE_##T)                                       \
+        return false;                                                                 \
+    }                                                                                 \
+    }

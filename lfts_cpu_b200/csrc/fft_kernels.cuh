@@ -1,0 +1,582 @@
+// Fused contour-step kernels for sm_100a.
+//
+// One contour step of the reference (step::fwd, src/step.cc:35-65) is
+//     q_{i+1} = h .* IFFT3( g .* FFT3(q_i) )
+// for two chains at once.  Here a 3-D transform is split into
+//   * a yz-plane pass (one CTA per x-plane per chain): inverse y, inverse z
+//     (complex-to-real), multiply by h, store q_{i+1}, forward z
+//     (real-to-complex), forward y -- i.e. the end of step i and the start of
+//     step i+1 fused, with the whole plane's half spectrum resident in shared
+//     memory (my x (mz/2+1) complex values);
+//   * an x-pencil pass (one CTA per tile of (ky,kz) columns per chain):
+//     forward x, multiply by g(k), inverse x.
+// Each 1-D transform of length n = R1*R2 runs as two in-register radix
+// stages separated by one shared-memory exchange: stage "A" works on the
+// strided sets {j2 + R2 t}, stage "B" on the contiguous blocks {R2 k1 + u}.
+// Running A then B leaves the data "transposed" (index k1 + R1 k2 stored at
+// R2 k1 + k2); running B then A takes it back to natural order.  Every stage
+// therefore works in place, and the order in between is only ever seen by
+// code that knows the mapping (ymap below).
+//
+// Two real rows of a plane are packed into one complex line (a + i b) for
+// the z transforms; the half spectra are separated / recombined with the
+// Hermitian symmetry X[n-k] = conj X[k].  As in FFTW's c2r, the imaginary
+// parts of the k=0 and k=n/2 coefficients are ignored on the way back.
+#pragma once
+#include "dft.cuh"
+
+namespace lfts {
+
+enum PlaneMode : int {
+    PLANE_INIT_W = 0,  // h = exp(-w/N) from the fields, store h, forward transform
+    PLANE_INIT_Q = 1,  // forward transform of given real rows (q_in or W-)
+    PLANE_STEP = 2,    // inverse, x h, store q, forward
+    PLANE_LAST = 3,    // inverse, x h, store q, partial sum of chain 0 (for Q)
+};
+
+template <typename T>
+struct PlaneArgs {
+    const double *w;      // INIT_W: W- (M) and w+ (M), FP64
+    const T *src;         // INIT_Q: source rows, chain c at src + c*src_stride
+    long long src_stride;
+    const double *src64;  // INIT_Q from FP64 rows (used when src == nullptr)
+    T *qout;              // stored propagators, chain c at qout + c*M
+    const T *h;           // [hA | hB]
+    cpx<T> *spec;         // half spectra, chain c at spec + c*mx*my*KZ
+    const cpx<T> *twy, *twz;  // exp(-2 pi i t/n) tables
+    double *qpart;        // LAST: per-plane sums of chain 0
+    int hsel0, hsel1;     // h half used by chain 0 / chain 1 (0 = hA, 1 = hB)
+    int nchains;
+    double Nd;            // N as a double (h = exp(-w/N))
+};
+
+template <typename T, int NY, int NZ>
+struct PlaneCfg {
+    static constexpr int KZ = NZ / 2 + 1;
+    static constexpr int RY1 = Plan<NY>::R1, RY2 = Plan<NY>::R2;
+    static constexpr int RZ1 = Plan<NZ>::R1, RZ2 = Plan<NZ>::R2;
+    static constexpr int PAIRS = NY / 2;
+    // Inside a row pair the packed z line is stored with one pad slot after
+    // every RZ2 slots (zpos), so the contiguous-block stages hit distinct
+    // shared-memory banks; the row pitch KZP leaves room for that.
+    static constexpr int ZSPAN = NZ + (NZ - 1) / RZ2;
+    static constexpr int KZP = KZ > (ZSPAN + 1) / 2 ? KZ : (ZSPAN + 1) / 2;
+    // The kz = 0 and kz = NZ/2 columns are real along y in real space, so they
+    // travel through the y transforms packed as one complex column (column 0:
+    // x = kz 0, y = kz NZ/2); the y phases work on KC = NZ/2 columns.
+    static constexpr int KC = NZ / 2;
+    // one thread per stage-A task of the y and z transforms (the larger of
+    // the two), so those phases take a single round; multiples of 4 warps
+    // keep the SM sub-partitions balanced
+    static constexpr int W0 = KC * RY2 > PAIRS * RZ2 ? KC * RY2 : PAIRS * RZ2;
+    static constexpr int W1 = (W0 + 127) / 128 * 128;
+    static constexpr int NT = W1 > 1024 ? 1024 : W1;
+    static constexpr size_t SMEM = sizeof(cpx<T>) * (size_t)(NY * KZP + 2 * NY + NZ);
+    // resident CTAs per SM the register budget is sized for (FP32 planes are
+    // small enough for two)
+    static constexpr int MINB = (sizeof(T) == 4 && 2 * SMEM < 200 * 1024 && NT <= 512) ? 2 : 1;
+    static_assert(NZ % 2 == 0 && NY % 2 == 0, "plane kernels need even my and mz");
+    static __device__ __forceinline__ int ymap(int p) { return p / RY2 + RY1 * (p % RY2); }
+    static __device__ __forceinline__ int zpos(int s) { return s + s / RZ2; }
+};
+
+template <int TASKS, int NT>
+struct Tpt {
+    static constexpr int v = (TASKS + NT - 1) / NT;
+};
+
+// ---------------------------------------------------------------- y phases --
+// inverse, natural -> transposed, stage A reading the global half spectrum
+template <typename C, typename T>
+__device__ __forceinline__ void y_invA_global(cpx<T> *P, const cpx<T> *__restrict__ Sg, const cpx<T> *twy)
+{
+    constexpr int KZ = C::KZ, KC = C::KC, KZP = C::KZP, R1 = C::RY1, R2 = C::RY2, NY = R1 * R2;
+    for (int t = threadIdx.x; t < KC * R2; t += C::NT) {
+        const int col = t % KC, j2 = t / KC;
+        cpx<T> v[R1];
+#pragma unroll
+        for (int a = 0; a < R1; a++) {
+            v[a] = Sg[(j2 + R2 * a) * KZ + col];
+            if (col == 0) {  // Y0 + i Y_{NZ/2}
+                const cpx<T> n2 = Sg[(j2 + R2 * a) * KZ + KC];
+                v[a] = {v[a].x - n2.y, v[a].y + n2.x};
+            }
+        }
+        Dft<R1, 1, T>::run(v);
+#pragma unroll
+        for (int k1 = 0; k1 < R1; k1++)
+            P[(j2 + R2 * k1) * KZP + col] = ctw<1>(v[k1], twy[(j2 * k1) % NY]);
+    }
+}
+
+// stage B in place with sign S; TW: apply exp(S 2pi i j2 k1/n) after the DFT
+template <typename C, int S, bool TW, typename T>
+__device__ __forceinline__ void y_B(cpx<T> *P, const cpx<T> *twy)
+{
+    constexpr int KC = C::KC, KZP = C::KZP, R1 = C::RY1, R2 = C::RY2, NY = R1 * R2;
+    for (int t = threadIdx.x; t < KC * R1; t += C::NT) {
+        const int col = t % KC, k1 = t / KC;
+        cpx<T> v[R2];
+#pragma unroll
+        for (int u = 0; u < R2; u++) v[u] = P[(R2 * k1 + u) * KZP + col];
+        Dft<R2, S, T>::run(v);
+#pragma unroll
+        for (int u = 0; u < R2; u++)
+            P[(R2 * k1 + u) * KZP + col] = TW ? ctw<S>(v[u], twy[(u * k1) % NY]) : v[u];
+    }
+}
+
+// forward, stage A in smem with twiddles (natural -> transposed start)
+template <typename C, typename T>
+__device__ __forceinline__ void y_fwdA_tw(cpx<T> *P, const cpx<T> *twy)
+{
+    constexpr int KC = C::KC, KZP = C::KZP, R1 = C::RY1, R2 = C::RY2, NY = R1 * R2;
+    for (int t = threadIdx.x; t < KC * R2; t += C::NT) {
+        const int col = t % KC, j2 = t / KC;
+        cpx<T> v[R1];
+#pragma unroll
+        for (int a = 0; a < R1; a++) v[a] = P[(j2 + R2 * a) * KZP + col];
+        Dft<R1, -1, T>::run(v);
+#pragma unroll
+        for (int k1 = 0; k1 < R1; k1++) P[(j2 + R2 * k1) * KZP + col] = ctw<-1>(v[k1], twy[(j2 * k1) % NY]);
+    }
+}
+
+// forward stage B -> global, natural order (end of natural -> natural forward)
+// (packed column 0 goes to colbuf for y_unpack0)
+template <typename C, typename T>
+__device__ __forceinline__ void y_fwdB_global(const cpx<T> *P, cpx<T> *__restrict__ Sg, cpx<T> *colbuf)
+{
+    constexpr int KZ = C::KZ, KC = C::KC, KZP = C::KZP, R1 = C::RY1, R2 = C::RY2;
+    for (int t = threadIdx.x; t < KC * R1; t += C::NT) {
+        const int col = t % KC, k1 = t / KC;
+        cpx<T> v[R2];
+#pragma unroll
+        for (int u = 0; u < R2; u++) v[u] = P[(R2 * k1 + u) * KZP + col];
+        Dft<R2, -1, T>::run(v);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; k2++) {
+            if (col == 0)
+                colbuf[k1 + R1 * k2] = v[k2];
+            else
+                Sg[(k1 + R1 * k2) * KZ + col] = v[k2];
+        }
+    }
+}
+
+// forward stage A -> global, natural order (end of transposed -> natural forward)
+template <typename C, typename T>
+__device__ __forceinline__ void y_fwdA_global(const cpx<T> *P, cpx<T> *__restrict__ Sg, cpx<T> *colbuf)
+{
+    constexpr int KZ = C::KZ, KC = C::KC, KZP = C::KZP, R1 = C::RY1, R2 = C::RY2;
+    for (int t = threadIdx.x; t < KC * R2; t += C::NT) {
+        const int col = t % KC, j2 = t / KC;
+        cpx<T> v[R1];
+#pragma unroll
+        for (int k1 = 0; k1 < R1; k1++) v[k1] = P[(j2 + R2 * k1) * KZP + col];
+        Dft<R1, -1, T>::run(v);
+#pragma unroll
+        for (int j1 = 0; j1 < R1; j1++) {
+            if (col == 0)
+                colbuf[j2 + R2 * j1] = v[j1];
+            else
+                Sg[(j2 + R2 * j1) * KZ + col] = v[j1];
+        }
+    }
+}
+
+// Separate the packed column Y = Y0 + i Y_{NZ/2} (natural ky order in colbuf)
+// into the kz = 0 and kz = NZ/2 columns of the global half spectrum.
+template <typename C, typename T>
+__device__ __forceinline__ void y_unpack0(const cpx<T> *colbuf, cpx<T> *__restrict__ Sg)
+{
+    constexpr int KZ = C::KZ, KC = C::KC, NY = C::RY1 * C::RY2;
+    for (int k = threadIdx.x; k < NY; k += C::NT) {
+        const cpx<T> z = colbuf[k], c = colbuf[(NY - k) % NY];
+        Sg[k * KZ] = {(T)0.5 * (z.x + c.x), (T)0.5 * (z.y - c.y)};
+        Sg[k * KZ + KC] = {(T)0.5 * (z.y + c.y), (T)-0.5 * (z.x - c.x)};
+    }
+}
+
+// ---------------------------------------------------------------- z phases --
+// Row pair q occupies the 2*KZP slots starting at P + 2q*KZP ("region");
+// the packed line's slot s lives at region[zpos(s)], the rows' k at row[k].
+
+// Build Z = A + iB (Hermitian-extended) and run inverse stage A.  Permuting:
+// all reads happen before a barrier, then all writes.
+template <typename C, typename T>
+__device__ __forceinline__ void z_build_invA(cpx<T> *P, const cpx<T> *twz)
+{
+    constexpr int KZP = C::KZP, R1 = C::RZ1, R2 = C::RZ2, NZ = R1 * R2;
+    constexpr int TASKS = C::PAIRS * R2;
+    constexpr int TPT = Tpt<TASKS, C::NT>::v;
+    cpx<T> hold[TPT][R1];
+#pragma unroll
+    for (int s = 0; s < TPT; s++) {
+        const int t = threadIdx.x + s * C::NT;
+        if (t < TASKS) {
+            const int q = t / R2, j2 = t % R2;
+            const cpx<T> *A = P + 2 * q * KZP, *B = A + KZP;
+#pragma unroll
+            for (int a = 0; a < R1; a++) {
+                const int k = j2 + R2 * a;
+                cpx<T> z;
+                if (k == 0) {
+                    z = {A[0].x, B[0].x};
+                } else if (2 * k == NZ) {
+                    z = {A[0].y, B[0].y};  // packed kz = NZ/2 (real part only, as c2r)
+                } else if (2 * k < NZ) {
+                    const cpx<T> av = A[k], bv = B[k];
+                    z = {av.x - bv.y, av.y + bv.x};
+                } else {
+                    const cpx<T> av = A[NZ - k], bv = B[NZ - k];
+                    z = {av.x + bv.y, bv.x - av.y};
+                }
+                hold[s][a] = z;
+            }
+            Dft<R1, 1, T>::run(hold[s]);
+#pragma unroll
+            for (int k1 = 0; k1 < R1; k1++) hold[s][k1] = ctw<1>(hold[s][k1], twz[(j2 * k1) % NZ]);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < TPT; s++) {
+        const int t = threadIdx.x + s * C::NT;
+        if (t < TASKS) {
+            const int q = t / R2, j2 = t % R2;
+            cpx<T> *Z = P + 2 * q * KZP;
+#pragma unroll
+            for (int k1 = 0; k1 < R1; k1++) Z[C::zpos(j2 + R2 * k1)] = hold[s][k1];
+        }
+    }
+}
+
+// Inverse stage B -> real rows (transposed z order), times h, store q;
+// STEP: then forward stage B with twiddles back into smem.
+// LAST: accumulate chain-0 values into *qsum instead.
+template <typename C, int MODE, typename T>
+__device__ __forceinline__ void z_invB_h(cpx<T> *P, const cpx<T> *twz, const T *__restrict__ h,
+                                         T *__restrict__ qrow, double &qsum)
+{
+    constexpr int KZP = C::KZP, R1 = C::RZ1, R2 = C::RZ2, NZ = R1 * R2;
+    for (int t = threadIdx.x; t < C::PAIRS * R1; t += C::NT) {
+        const int q = t / R1, k1 = t % R1;
+        cpx<T> *Z = P + 2 * q * KZP;
+        const int ya = C::ymap(2 * q), yb = C::ymap(2 * q + 1);
+        cpx<T> v[R2];
+#pragma unroll
+        for (int u = 0; u < R2; u++) v[u] = Z[C::zpos(R2 * k1 + u)];
+        Dft<R2, 1, T>::run(v);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; k2++) {
+            const int z = k1 + R1 * k2;
+            const T a = v[k2].x * h[ya * NZ + z];
+            const T b = v[k2].y * h[yb * NZ + z];
+            qrow[ya * NZ + z] = a;
+            qrow[yb * NZ + z] = b;
+            if (MODE == PLANE_LAST) qsum += (double)a + (double)b;
+            v[k2] = {a, b};
+        }
+        if (MODE == PLANE_STEP) {
+            Dft<R2, -1, T>::run(v);
+#pragma unroll
+            for (int u = 0; u < R2; u++) Z[C::zpos(R2 * k1 + u)] = ctw<-1>(v[u], twz[(u * k1) % NZ]);
+        }
+    }
+}
+
+// forward stage A, transposed -> natural, in place
+template <typename C, typename T>
+__device__ __forceinline__ void z_fwdA(cpx<T> *P)
+{
+    constexpr int KZP = C::KZP, R1 = C::RZ1, R2 = C::RZ2;
+    for (int t = threadIdx.x; t < C::PAIRS * R2; t += C::NT) {
+        const int q = t / R2, j2 = t % R2;
+        cpx<T> *Z = P + 2 * q * KZP;
+        cpx<T> v[R1];
+#pragma unroll
+        for (int k1 = 0; k1 < R1; k1++) v[k1] = Z[C::zpos(j2 + R2 * k1)];
+        Dft<R1, -1, T>::run(v);
+#pragma unroll
+        for (int j1 = 0; j1 < R1; j1++) Z[C::zpos(j2 + R2 * j1)] = v[j1];
+    }
+}
+
+// forward stage A with twiddles, natural -> (start of) transposed, in place
+template <typename C, typename T>
+__device__ __forceinline__ void z_fwdA_tw(cpx<T> *P, const cpx<T> *twz)
+{
+    constexpr int KZP = C::KZP, R1 = C::RZ1, R2 = C::RZ2, NZ = R1 * R2;
+    for (int t = threadIdx.x; t < C::PAIRS * R2; t += C::NT) {
+        const int q = t / R2, j2 = t % R2;
+        cpx<T> *Z = P + 2 * q * KZP;
+        cpx<T> v[R1];
+#pragma unroll
+        for (int a = 0; a < R1; a++) v[a] = Z[C::zpos(j2 + R2 * a)];
+        Dft<R1, -1, T>::run(v);
+#pragma unroll
+        for (int k1 = 0; k1 < R1; k1++) Z[C::zpos(j2 + R2 * k1)] = ctw<-1>(v[k1], twz[(j2 * k1) % NZ]);
+    }
+}
+
+// forward stage B without twiddles, in place (ends natural -> transposed)
+template <typename C, typename T>
+__device__ __forceinline__ void z_fwdB(cpx<T> *P)
+{
+    constexpr int KZP = C::KZP, R1 = C::RZ1, R2 = C::RZ2;
+    for (int t = threadIdx.x; t < C::PAIRS * R1; t += C::NT) {
+        const int q = t / R1, k1 = t % R1;
+        cpx<T> *Z = P + 2 * q * KZP;
+        cpx<T> v[R2];
+#pragma unroll
+        for (int u = 0; u < R2; u++) v[u] = Z[C::zpos(R2 * k1 + u)];
+        Dft<R2, -1, T>::run(v);
+#pragma unroll
+        for (int u = 0; u < R2; u++) Z[C::zpos(R2 * k1 + u)] = v[u];
+    }
+}
+
+// Separate the packed spectrum Z of rows (a, b) into the half spectra A, B.
+// TRANSPOSED: Z[k] sits at R2*(k % R1) + k / R1, else at k.  Permuting.
+template <typename C, bool TRANSPOSED, typename T>
+__device__ __forceinline__ void z_unpack(cpx<T> *P)
+{
+    constexpr int KC = C::KC, KZP = C::KZP, R1 = C::RZ1, R2 = C::RZ2, NZ = R1 * R2;
+    constexpr int TASKS = C::PAIRS * KC;
+    constexpr int TPT = Tpt<TASKS, C::NT>::v;
+    cpx<T> ha[TPT], hb[TPT];
+#pragma unroll
+    for (int s = 0; s < TPT; s++) {
+        const int t = threadIdx.x + s * C::NT;
+        if (t < TASKS) {
+            const int q = t / KC, k = t % KC;
+            const int nk = (k == 0) ? NZ / 2 : NZ - k;  // k = 0 pairs DC with Nyquist
+            const cpx<T> *Z = P + 2 * q * KZP;
+            const int pk = TRANSPOSED ? R2 * (k % R1) + k / R1 : k;
+            const int pn = TRANSPOSED ? R2 * (nk % R1) + nk / R1 : nk;
+            const cpx<T> z = Z[C::zpos(pk)], c = Z[C::zpos(pn)];
+            if (k == 0) {
+                // A[0], A[NZ/2], B[0], B[NZ/2] are real: A = Re Z, B = Im Z
+                ha[s] = {z.x, c.x};
+                hb[s] = {z.y, c.y};
+            } else {
+                // A = (z + conj c)/2, B = (z - conj c)/(2i)
+                ha[s] = {(T)0.5 * (z.x + c.x), (T)0.5 * (z.y - c.y)};
+                hb[s] = {(T)0.5 * (z.y + c.y), (T)-0.5 * (z.x - c.x)};
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < TPT; s++) {
+        const int t = threadIdx.x + s * C::NT;
+        if (t < TASKS) {
+            const int q = t / KC, k = t % KC;
+            P[2 * q * KZP + k] = ha[s];
+            P[(2 * q + 1) * KZP + k] = hb[s];
+        }
+    }
+}
+
+template <typename C, typename T>
+__device__ __forceinline__ void load_tw(cpx<T> *dst, const cpx<T> *__restrict__ src, int n)
+{
+    for (int t = threadIdx.x; t < n; t += C::NT) dst[t] = src[t];
+}
+
+// ------------------------------------------------------------ plane kernel --
+template <typename T, int NY, int NZ, int MODE>
+__global__ void __launch_bounds__(PlaneCfg<T, NY, NZ>::NT, PlaneCfg<T, NY, NZ>::MINB) plane_kernel(PlaneArgs<T> a)
+{
+    using C = PlaneCfg<T, NY, NZ>;
+    constexpr int KZ = C::KZ, KZP = C::KZP;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<T> *P = reinterpret_cast<cpx<T> *>(smem_raw);
+    cpx<T> *twy = P + NY * KZP;
+    cpx<T> *twz = twy + NY;
+    cpx<T> *colbuf = twz + NZ;
+
+    const int x = blockIdx.x, c = blockIdx.y;
+    const int mx = gridDim.x;
+    const long long M = (long long)mx * NY * NZ;
+    const long long plane_off = (long long)x * NY * NZ;
+    cpx<T> *Sg = a.spec + ((long long)c * mx + x) * NY * KZ;
+
+    load_tw<C>(twy, a.twy, NY);
+    load_tw<C>(twz, a.twz, NZ);
+
+    if (MODE == PLANE_INIT_W || MODE == PLANE_INIT_Q) {
+        // real rows (natural y order), packed two per complex line
+        for (int t = threadIdx.x; t < C::PAIRS * NZ; t += C::NT) {
+            const int q = t / NZ, z = t % NZ;
+            const long long ia = plane_off + (2 * q) * NZ + z, ib = ia + NZ;
+            T va, vb;
+            if (MODE == PLANE_INIT_W) {
+                // hA = exp(-(W- + w+)/N), hB = exp(-(-W- + w+)/N)  (src/diblock.cc:64-72)
+                const double sgn = c == 0 ? 1.0 : -1.0;
+                const double da = exp(-(sgn * a.w[ia] + a.w[M + ia]) / a.Nd);
+                const double db = exp(-(sgn * a.w[ib] + a.w[M + ib]) / a.Nd);
+                va = (T)da;
+                vb = (T)db;
+                a.qout[c * M + ia] = va;
+                a.qout[c * M + ib] = vb;
+            } else if (a.src) {
+                va = a.src[c * a.src_stride + ia];
+                vb = a.src[c * a.src_stride + ib];
+            } else {
+                va = (T)a.src64[c * a.src_stride + ia];
+                vb = (T)a.src64[c * a.src_stride + ib];
+            }
+            P[2 * q * KZP + C::zpos(z)] = {va, vb};
+        }
+        __syncthreads();
+        z_fwdA_tw<C>(P, twz);
+        __syncthreads();
+        z_fwdB<C>(P);
+        __syncthreads();
+        z_unpack<C, true>(P);
+        __syncthreads();
+        y_fwdA_tw<C>(P, twy);
+        __syncthreads();
+        y_fwdB_global<C>(P, Sg, colbuf);
+        __syncthreads();
+        y_unpack0<C>(colbuf, Sg);
+        return;
+    }
+
+    // inverse y (natural -> transposed rows), then packed z lines
+    __syncthreads();
+    y_invA_global<C>(P, Sg, twy);
+    __syncthreads();
+    y_B<C, 1, false>(P, twy);
+    __syncthreads();
+    z_build_invA<C>(P, twz);
+    __syncthreads();
+    const T *h = a.h + (long long)(c == 0 ? a.hsel0 : a.hsel1) * M + plane_off;
+    T *qrow = a.qout + c * M + plane_off;
+    double qsum = 0.0;
+    z_invB_h<C, MODE>(P, twz, h, qrow, qsum);
+    if (MODE == PLANE_LAST) {
+        if (c == 0) {
+            // deterministic block reduction of the plane sum
+            __shared__ double red[C::NT / 32];
+            for (int o = 16; o > 0; o >>= 1) qsum += __shfl_xor_sync(0xffffffffu, qsum, o);
+            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = qsum;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double s = 0.0;
+                for (int i = 0; i < C::NT / 32; i++) s += red[i];
+                a.qpart[x] = s;
+            }
+        }
+        return;
+    }
+    __syncthreads();
+    z_fwdA<C>(P);
+    __syncthreads();
+    z_unpack<C, false>(P);
+    __syncthreads();
+    y_B<C, -1, true>(P, twy);
+    __syncthreads();
+    y_fwdA_global<C>(P, Sg, colbuf);
+    __syncthreads();
+    y_unpack0<C>(colbuf, Sg);
+}
+
+// ----------------------------------------------------------- pencil kernel --
+enum PencilMode : int {
+    PENCIL_CONV = 0,  // forward x, times g, inverse x (in place in the spectrum)
+    PENCIL_POWER = 1, // forward x, S += |X|^2 (structure function sample)
+};
+
+template <typename T>
+struct PencilArgs {
+    cpx<T> *spec;             // chain c at spec + c*mx*ncol
+    const cpx<T> *twx;        // exp(-2 pi i t/mx)
+    const T *gx, *gy, *gz;    // separable Boltzmann weight, 1/M folded into gz
+    double *S;                // POWER: accumulator (mx*ncol)
+    int ncol;                 // my*KZ
+    int KZ;
+};
+
+template <typename T, int NX, int CW>
+struct PencilCfg {
+    static constexpr int R1 = Plan<NX>::R1, R2 = Plan<NX>::R2;
+    static constexpr int W0 = CW * (R1 > R2 ? R1 : R2);
+    static constexpr int NT = W0 >= 512 ? 256 : (W0 <= 128 ? 128 : 256);
+    static constexpr size_t SMEM = sizeof(cpx<T>) * (size_t)(NX * CW + NX) + sizeof(T) * NX;
+};
+
+template <typename T, int NX, int CW, int MODE>
+__global__ void __launch_bounds__(PencilCfg<T, NX, CW>::NT) pencil_kernel(PencilArgs<T> a)
+{
+    using C = PencilCfg<T, NX, CW>;
+    constexpr int R1 = C::R1, R2 = C::R2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<T> *Tl = reinterpret_cast<cpx<T> *>(smem_raw);
+    cpx<T> *twx = Tl + NX * CW;
+    T *gxs = reinterpret_cast<T *>(twx + NX);
+
+    const int col0 = blockIdx.x * CW, c = blockIdx.y;
+    const int ncol = a.ncol;
+    cpx<T> *Sg = a.spec + (long long)c * NX * ncol;
+    for (int t = threadIdx.x; t < NX; t += C::NT) {
+        twx[t] = a.twx[t];
+        if (MODE == PENCIL_CONV) gxs[t] = a.gx[t];  // POWER mode has no g table
+    }
+    __syncthreads();
+
+    // X1: forward stage A from global (strided rows), twiddles, to smem
+    for (int t = threadIdx.x; t < CW * R2; t += C::NT) {
+        const int cl = t % CW, j2 = t / CW, col = col0 + cl;
+        if (col >= ncol) continue;
+        cpx<T> v[R1];
+#pragma unroll
+        for (int s = 0; s < R1; s++) v[s] = Sg[(long long)(j2 + R2 * s) * ncol + col];
+        Dft<R1, -1, T>::run(v);
+#pragma unroll
+        for (int k1 = 0; k1 < R1; k1++) Tl[(j2 + R2 * k1) * CW + cl] = ctw<-1>(v[k1], twx[(j2 * k1) % NX]);
+    }
+    __syncthreads();
+
+    // X2: forward stage B -> X[k1 + R1 k2]; then g and inverse stage B, or |X|^2
+    for (int t = threadIdx.x; t < CW * R1; t += C::NT) {
+        const int cl = t % CW, k1 = t / CW, col = col0 + cl;
+        if (col >= ncol) continue;
+        cpx<T> v[R2];
+#pragma unroll
+        for (int u = 0; u < R2; u++) v[u] = Tl[(R2 * k1 + u) * CW + cl];
+        Dft<R2, -1, T>::run(v);
+        if (MODE == PENCIL_CONV) {
+            const T gyz = a.gy[col / a.KZ] * a.gz[col % a.KZ];
+#pragma unroll
+            for (int k2 = 0; k2 < R2; k2++) v[k2] = cscale(v[k2], gxs[k1 + R1 * k2] * gyz);
+            Dft<R2, 1, T>::run(v);
+#pragma unroll
+            for (int u = 0; u < R2; u++) Tl[(R2 * k1 + u) * CW + cl] = ctw<1>(v[u], twx[(u * k1) % NX]);
+        } else {
+#pragma unroll
+            for (int k2 = 0; k2 < R2; k2++) {
+                const long long o = (long long)(k1 + R1 * k2) * ncol + col;
+                a.S[o] += (double)v[k2].x * (double)v[k2].x + (double)v[k2].y * (double)v[k2].y;
+            }
+        }
+    }
+    if (MODE == PENCIL_POWER) return;
+    __syncthreads();
+
+    // X3: inverse stage A (strided) -> natural order, to global
+    for (int t = threadIdx.x; t < CW * R2; t += C::NT) {
+        const int cl = t % CW, j2 = t / CW, col = col0 + cl;
+        if (col >= ncol) continue;
+        cpx<T> v[R1];
+#pragma unroll
+        for (int k1 = 0; k1 < R1; k1++) v[k1] = Tl[(j2 + R2 * k1) * CW + cl];
+        Dft<R1, 1, T>::run(v);
+#pragma unroll
+        for (int j1 = 0; j1 < R1; j1++) Sg[(long long)(j2 + R2 * j1) * ncol + col] = v[j1];
+    }
+}
+
+}  // namespace lfts

@@ -1,0 +1,204 @@
+// Streaming kernels around the contour steps: concentrations (with the
+// Anderson residual and its dot products fused in), the Anderson w+ update,
+// the Langevin W- update, S(k) spherical binning and the H sums.
+//
+// The element-wise updates reproduce the reference's expression trees with
+// explicitly rounded operations (__dadd_rn etc.), so no multiply-add is
+// contracted and a GPU element equals the reference's element bit for bit
+// given equal inputs.  Reductions are deterministic: fixed grid, fixed
+// per-block tree, fixed-order final pass.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace lfts {
+
+constexpr int kMaxHist = 10;          // anderson(M_, 10) (src/lfts_simulation.cc:34)
+constexpr int kRedWidth = kMaxHist + 1;
+constexpr int kRedThreads = 256;
+
+struct HistPtrs {
+    const double *p[kMaxHist];
+};
+struct Coefs {
+    double c[kMaxHist];
+};
+
+// sum of v over the block; result valid in thread 0
+__device__ __forceinline__ double block_sum(double v, double *sh)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) s += sh[i];
+    return s;
+}
+
+// Q = sum(qpart)/M and ln Q (src/diblock.cc:46-48,59)
+__global__ void q_finalize_kernel(const double *qpart, int n, long long M, double *Q_out)
+{
+    __shared__ double sh[32];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += qpart[i];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) {
+        const double Q = s / (double)M;
+        Q_out[0] = Q;
+        Q_out[1] = log(Q);
+    }
+}
+
+// phi-/phi+ (src/diblock.cc:50-57, 85-95) and, when Dh0 != nullptr, the
+// Anderson residual Dh0 = phi+ - 1 with partial sums of Dh0*Dh0 and
+// Dh0*Dh_m, m = 1..nh (src/anderson.cc:35-55).
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) concentrations_kernel(
+    const T *__restrict__ q, long long M, int N, int NA, const double *__restrict__ w,
+    double *__restrict__ phim, double *__restrict__ phip, const double *__restrict__ Qd,
+    double *__restrict__ Dh0, int nh, HistPtrs hist, double *__restrict__ partials)
+{
+    __shared__ double sh[kRedThreads / 32];
+    const double Q = Qd[0];
+    const double NQ = __dmul_rn((double)N, Q);
+    double acc[kRedWidth];
+#pragma unroll
+    for (int m = 0; m < kRedWidth; m++) acc[m] = 0.0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < M; r += stride) {
+        // slot i holds [q_i | q^_{N+1-i}] (src/diblock.cc:19-24); slot i at q + (i-1)*2M
+        double sA = 0.0, sB = 0.0;
+        for (int i = 1; i <= N; i++) {
+            const double a = (double)q[(long long)(i - 1) * 2 * M + r];
+            const double b = (double)q[(long long)(N - i) * 2 * M + M + r];
+            if (i <= NA)
+                sA = __dadd_rn(sA, __dmul_rn(a, b));
+            else
+                sB = __dadd_rn(sB, __dmul_rn(a, b));
+        }
+        const double wm = w[r], wp = w[M + r];
+        const double hA = exp(-(wm + wp) / (double)N);
+        const double hB = exp(-(-wm + wp) / (double)N);
+        const double fA = sA / __dmul_rn(NQ, hA);
+        const double fB = sB / __dmul_rn(NQ, hB);
+        const double pm = __dsub_rn(fA, fB), pp = __dadd_rn(fA, fB);
+        phim[r] = pm;
+        phip[r] = pp;
+        if (Dh0) {
+            const double d = __dsub_rn(pp, 1.0);
+            Dh0[r] = d;
+            acc[0] = __dadd_rn(acc[0], __dmul_rn(d, d));
+#pragma unroll
+            for (int m = 1; m < kRedWidth; m++)
+                if (m <= nh) acc[m] = __dadd_rn(acc[m], __dmul_rn(d, hist.p[m - 1][r]));
+        }
+    }
+    if (!Dh0) return;
+#pragma unroll
+    for (int m = 0; m < kRedWidth; m++) {
+        if (m > nh) break;
+        const double s = block_sum(acc[m], sh);
+        if (threadIdx.x == 0) partials[(long long)blockIdx.x * kRedWidth + m] = s;
+    }
+}
+
+// out[m] = sum over blocks of partials[b][m], m < width, fixed order
+__global__ void reduce_partials_kernel(const double *partials, int nblocks, int width, double *out)
+{
+    __shared__ double sh[32];
+    for (int m = 0; m < width; m++) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += partials[(long long)b * kRedWidth + m];
+        s = block_sum(s, sh);
+        if (threadIdx.x == 0) out[m] = s;
+    }
+}
+
+// w+ update of one Anderson iteration (src/anderson.cc:57-79) and the copy
+// of the pre-update w+ into the current history slot (wh_[0], :38).
+__global__ void anderson_update_kernel(double *__restrict__ wp, double *__restrict__ wh0,
+                                       const double *__restrict__ Dh0, long long M, double lambda,
+                                       int nh, int simple, HistPtrs Dh, HistPtrs wh, Coefs C)
+{
+    const double *c = C.c;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < M; r += stride) {
+        const double old = wp[r];
+        const double d0 = Dh0[r];
+        wh0[r] = old;
+        const double base = __dadd_rn(old, __dmul_rn(lambda, d0));
+        double acc = base;
+        if (!simple) {
+#pragma unroll
+            for (int n = 0; n < kMaxHist; n++) {
+                if (n < nh) {
+                    const double hn = __dadd_rn(wh.p[n][r], __dmul_rn(lambda, Dh.p[n][r]));
+                    acc = __dadd_rn(acc, __dmul_rn(c[n], __dsub_rn(hn, base)));
+                }
+            }
+        }
+        wp[r] = acc;
+    }
+}
+
+// W- += -(phi- + 2 W-/XbN) dt + (eta_prev + eta_new)/2   (src/langevin.cc:31)
+__global__ void langevin_kernel(double *__restrict__ w, long long M, const double *__restrict__ eta_prev,
+                                const double *__restrict__ eta_new, double XbN, double dt)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < M; r += stride) {
+        const double wm = w[r], pm = w[2 * M + r];
+        const double drift = __dmul_rn(-__dadd_rn(pm, __ddiv_rn(__dmul_rn(2.0, wm), XbN)), dt);
+        const double noise = __dmul_rn(0.5, __dadd_rn(eta_prev[r], eta_new[r]));
+        w[r] = __dadd_rn(wm, __dadd_rn(drift, noise));
+    }
+}
+
+// partial sums of w+ and W-^2 (src/lfts_simulation.cc:129-131)
+__global__ void __launch_bounds__(kRedThreads) h_sums_kernel(const double *__restrict__ w, long long M,
+                                                             double *partials)
+{
+    __shared__ double sh[kRedThreads / 32];
+    double sp = 0.0, s2 = 0.0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < M; r += stride) {
+        const double wm = w[r];
+        sp += w[M + r];
+        s2 += wm * wm;
+    }
+    sp = block_sum(sp, sh);
+    if (threadIdx.x == 0) partials[(long long)blockIdx.x * kRedWidth + 0] = sp;
+    s2 = block_sum(s2, sh);
+    if (threadIdx.x == 0) partials[(long long)blockIdx.x * kRedWidth + 1] = s2;
+}
+
+// Spherical average of S(k) (src/strFunc.cc:50-76): one thread per |K| bin,
+// summing its wavevectors in the reference's stable-sorted order.
+__global__ void sk_bin_kernel(const double *__restrict__ S, const int *__restrict__ order,
+                              const int *__restrict__ wt, const int *__restrict__ bin_start, int nbins,
+                              double coeff_over_ns, double half_over_chi, double *__restrict__ out)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nbins) return;
+    double s = 0.0;
+    int n = 0;
+    for (int k = bin_start[b]; k < bin_start[b + 1]; k++) {
+        const int p = order[k];
+        const double term = __dsub_rn(__dmul_rn(coeff_over_ns, S[p]), half_over_chi);
+        s = __dadd_rn(s, __dmul_rn((double)wt[p], term));
+        n += wt[p];
+    }
+    out[b] = s / (double)n;
+}
+
+template <typename Tin, typename Tout>
+__global__ void convert_kernel(const Tin *__restrict__ in, Tout *__restrict__ out, long long n)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        out[i] = (Tout)in[i];
+}
+
+}  // namespace lfts

@@ -1,0 +1,990 @@
+// C ABI of the B200 L-FTS step (include/lfts_b200.h): device state, launch
+// orchestration and the small host-side pieces (Anderson least squares,
+// S(k) bin tables) around the kernels in fft_kernels.cuh / field_kernels.cuh.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/lfts_b200.h"
+#include "fft_dispatch.h"
+#include "field_kernels.cuh"
+
+using namespace lfts;
+
+namespace {
+
+thread_local std::string g_last_error = "";
+
+int cuda_fail(cudaError_t e, const char *what)
+{
+    char buf[512];
+    snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+    g_last_error = buf;
+    return LFTS_ERR_CUDA;
+}
+
+#define CK(call)                                           \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+constexpr double kTwoPi = 6.283185307179586476925286766559005768;
+
+// Gaussian elimination with partial pivoting (first maximal |pivot|,
+// reciprocal scaling of the sub-column, right-looking rank-1 updates), then
+// forward/back substitution: the LU solve the reference does with GSL at
+// src/anderson.cc:106-127.  Returns false for an exactly singular matrix,
+// where GSL's solve reports an error.
+bool lu_solve(std::vector<double> A, std::vector<double> y, double *x, int n)
+{
+    std::vector<int> perm(n);
+    std::iota(perm.begin(), perm.end(), 0);
+    for (int j = 0; j < n; j++) {
+        int piv = j;
+        double amax = std::fabs(A[j * n + j]);
+        for (int i = j + 1; i < n; i++) {
+            double v = std::fabs(A[i * n + j]);
+            if (v > amax) { amax = v; piv = i; }
+        }
+        if (piv != j) {
+            for (int k = 0; k < n; k++) std::swap(A[j * n + k], A[piv * n + k]);
+            std::swap(perm[j], perm[piv]);
+        }
+        if (j + 1 < n) {
+            const double ajj = A[j * n + j];
+            if (std::fabs(ajj) >= 2.2250738585072014e-308) {
+                const double inv = 1.0 / ajj;
+                for (int i = j + 1; i < n; i++) A[i * n + j] *= inv;
+            } else {
+                for (int i = j + 1; i < n; i++) A[i * n + j] /= ajj;
+            }
+            for (int i = j + 1; i < n; i++) {
+                const double lij = A[i * n + j];
+                for (int k = j + 1; k < n; k++) A[i * n + k] -= lij * A[j * n + k];
+            }
+        }
+    }
+    for (int i = 0; i < n; i++)
+        if (A[i * n + i] == 0.0) return false;
+    for (int i = 0; i < n; i++) x[i] = y[perm[i]];
+    for (int i = 0; i < n; i++) {
+        double t = x[i];
+        for (int j = 0; j < i; j++) t -= A[i * n + j] * x[j];
+        x[i] = t;
+    }
+    for (int i = n - 1; i >= 0; i--) {
+        double t = x[i];
+        for (int j = i + 1; j < n; j++) t -= A[i * n + j] * x[j];
+        x[i] = t / A[i * n + i];
+    }
+    return true;
+}
+
+// signed wavenumber of index K in [0, m): -(m-1)/2 .. m/2 (src/step.cc:69-79)
+inline int signed_k(int K, int m) { return (K <= m / 2) ? K : K - m; }
+
+}  // namespace
+
+struct lfts_ctx {
+    lfts_params p{};
+    int prec = 0, dev = 0;
+    int N = 0, NA = 0, NB = 0;
+    int mx = 0, my = 0, mz = 0, KZ = 0;
+    long long M = 0, Mk = 0;
+    size_t tsize = 8;  // bytes of the propagator type
+    cudaStream_t st = nullptr;
+    int sms = 148;
+
+    double *w = nullptr;       // 4M: W-, w+, phi-, phi+
+    void *q = nullptr;         // N slots x 2M, slot i at (i-1)*2M
+    void *spec = nullptr;      // 2 x mx x my x KZ complex
+    void *tw[3] = {};          // exp(-2 pi i t/m) per dimension
+    void *gtab[3] = {};        // gx[mx], gy[my], gz[KZ] (gz carries 1/M)
+    double *qpart = nullptr;   // mx per-plane sums of q_N
+    double *Qd = nullptr;      // Q, ln Q
+    double *partials = nullptr;
+    double *red = nullptr;     // kRedWidth reduced values (device)
+    double *red_host = nullptr;  // pinned copy
+    int red_blocks = 0;
+
+    double *eta[2] = {};       // Langevin noise: prev, new
+    int eta_prev = 0;
+    bool eta_set = false;
+
+    double *Dh[kRedWidth] = {}, *wh[kRedWidth] = {};  // Anderson ring (physical buffers)
+    int phys[kRedWidth] = {};  // logical history slot -> physical buffer
+    int cur = 0;               // physical buffer of the current iteration
+    double DD[kRedWidth][kRedWidth] = {};
+
+    double *S = nullptr;       // S(k) accumulator (Mk)
+    void *skspec = nullptr;    // FP64 spectrum scratch for S(k)
+    bool sk_own_spec = false;
+    void *sktw[3] = {};        // FP64 twiddles (FP32 contexts only)
+    int nsamples = 0;
+    double sk_dK = -1.0;
+    int sk_nbins = 0;
+    int *sk_order = nullptr, *sk_wt = nullptr, *sk_bins = nullptr;
+    double *sk_out = nullptr;
+    std::vector<double> sk_K;  // K value reported for each bin
+
+    void *sf_buf = nullptr;    // step_fwd scratch: q_in, q_out, h (2M each, FP64)
+
+    PlaneKernels<double> pl64{};
+    PencilKernels<double> pe64{};
+    PlaneKernels<float> pl32{};
+    PencilKernels<float> pe32{};
+
+    bool fields_set = false;
+    bool have_concs = false;
+    long long launches = 0;
+    long long mix_calls = 0, mix_iters = 0;
+};
+
+namespace {
+
+template <typename T>
+PlaneKernels<T> &plane_of(lfts_ctx *c);
+template <>
+PlaneKernels<double> &plane_of<double>(lfts_ctx *c) { return c->pl64; }
+template <>
+PlaneKernels<float> &plane_of<float>(lfts_ctx *c) { return c->pl32; }
+template <typename T>
+PencilKernels<T> &pencil_of(lfts_ctx *c);
+template <>
+PencilKernels<double> &pencil_of<double>(lfts_ctx *c) { return c->pe64; }
+template <>
+PencilKernels<float> &pencil_of<float>(lfts_ctx *c) { return c->pe32; }
+
+template <typename T>
+int set_smem_attrs(const PlaneKernels<T> &pl, const PencilKernels<T> &pe)
+{
+    for (int m = 0; m < 4; m++)
+        CK(cudaFuncSetAttribute(pl.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
+    for (int m = 0; m < 2; m++)
+        CK(cudaFuncSetAttribute(pe.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pe.smem));
+    return LFTS_OK;
+}
+
+template <typename T>
+int upload_tables(lfts_ctx *c, void **tw, void **gt)
+{
+    const int m[3] = {c->mx, c->my, c->mz};
+    for (int d = 0; d < 3; d++) {
+        std::vector<cpx<T>> t(m[d]);
+        for (int k = 0; k < m[d]; k++) {
+            long double a = -(long double)kTwoPi * (long double)k / (long double)m[d];
+            t[k].x = (T)(double)cosl(a);
+            t[k].y = (T)(double)sinl(a);
+        }
+        CK(cudaMalloc(&tw[d], sizeof(cpx<T>) * m[d]));
+        CK(cudaMemcpy(tw[d], t.data(), sizeof(cpx<T>) * m[d], cudaMemcpyHostToDevice));
+    }
+    if (!gt) return LFTS_OK;
+    // g = exp(-(2 pi)^2 (kx^2/Lx^2 + ky^2/Ly^2 + kz^2/Lz^2)/(6N)) / M, factorised
+    const int n[3] = {c->mx, c->my, c->KZ};
+    for (int d = 0; d < 3; d++) {
+        std::vector<T> g(n[d]);
+        for (int K = 0; K < n[d]; K++) {
+            const int k = (d == 2) ? K : signed_k(K, m[d]);
+            const double ksq = (double)k * k / (c->p.L[d] * c->p.L[d]);
+            double v = std::exp(-kTwoPi * kTwoPi * ksq / (6.0 * c->N));
+            if (d == 2) v /= (double)c->M;
+            g[K] = (T)v;
+        }
+        CK(cudaMalloc(&gt[d], sizeof(T) * n[d]));
+        CK(cudaMemcpy(gt[d], g.data(), sizeof(T) * n[d], cudaMemcpyHostToDevice));
+    }
+    return LFTS_OK;
+}
+
+inline dim3 stream_grid(const lfts_ctx *c) { return dim3(c->red_blocks); }
+
+// ---- contour chain ----------------------------------------------------------
+template <typename T>
+PlaneArgs<T> plane_args(lfts_ctx *c)
+{
+    PlaneArgs<T> a{};
+    a.w = c->w;
+    a.spec = static_cast<cpx<T> *>(c->spec);
+    a.twy = static_cast<const cpx<T> *>(c->tw[1]);
+    a.twz = static_cast<const cpx<T> *>(c->tw[2]);
+    a.qpart = c->qpart;
+    a.nchains = 2;
+    a.Nd = (double)c->N;
+    return a;
+}
+
+template <typename T>
+PencilArgs<T> pencil_args(lfts_ctx *c)
+{
+    PencilArgs<T> a{};
+    a.spec = static_cast<cpx<T> *>(c->spec);
+    a.twx = static_cast<const cpx<T> *>(c->tw[0]);
+    a.gx = static_cast<const T *>(c->gtab[0]);
+    a.gy = static_cast<const T *>(c->gtab[1]);
+    a.gz = static_cast<const T *>(c->gtab[2]);
+    a.ncol = c->my * c->KZ;
+    a.KZ = c->KZ;
+    return a;
+}
+
+template <typename T>
+void launch_plane(lfts_ctx *c, int mode, const PlaneArgs<T> &a, int nchains)
+{
+    const PlaneKernels<T> &pl = plane_of<T>(c);
+    pl.fn[mode]<<<dim3(c->mx, nchains), pl.nt, pl.smem, c->st>>>(a);
+    c->launches++;
+}
+
+template <typename T>
+void launch_pencil(lfts_ctx *c, int mode, const PencilArgs<T> &a, int nchains)
+{
+    const PencilKernels<T> &pe = pencil_of<T>(c);
+    const int ncol = c->my * c->KZ;
+    pe.fn[mode]<<<dim3((ncol + pe.cw - 1) / pe.cw, nchains), pe.nt, pe.smem, c->st>>>(a);
+    c->launches++;
+}
+
+inline int hsel_chain0(const lfts_ctx *c, int i) { return i < c->NA ? 0 : 1; }  // src/step.cc:53-57
+inline int hsel_chain1(const lfts_ctx *c, int i) { return i < c->NB ? 1 : 0; }  // src/step.cc:60-64
+
+// propagators of both chains for all N monomers, then Q (src/diblock.cc:36-48)
+template <typename T>
+void enqueue_chain(lfts_ctx *c)
+{
+    T *q = static_cast<T *>(c->q);
+    const long long M = c->M;
+    PlaneArgs<T> a = plane_args<T>(c);
+    a.qout = q;  // slot 1 = [hA | hB]
+    launch_plane<T>(c, PLANE_INIT_W, a, 2);
+    PencilArgs<T> pa = pencil_args<T>(c);
+    a.h = q;
+    for (int i = 1; i < c->N; i++) {
+        launch_pencil<T>(c, PENCIL_CONV, pa, 2);
+        a.qout = q + (long long)i * 2 * M;  // slot i+1
+        a.hsel0 = hsel_chain0(c, i);
+        a.hsel1 = hsel_chain1(c, i);
+        launch_plane<T>(c, i + 1 < c->N ? PLANE_STEP : PLANE_LAST, a, 2);
+    }
+    q_finalize_kernel<<<1, 256, 0, c->st>>>(c->qpart, c->mx, M, c->Qd);
+    c->launches++;
+}
+
+template <typename T>
+void enqueue_concs(lfts_ctx *c, double *Dh0, int nh, const HistPtrs &hist)
+{
+    enqueue_chain<T>(c);
+    concentrations_kernel<T><<<stream_grid(c), kRedThreads, 0, c->st>>>(
+        static_cast<const T *>(c->q), c->M, c->N, c->NA, c->w, c->w + 2 * c->M, c->w + 3 * c->M, c->Qd,
+        Dh0, nh, hist, c->partials);
+    c->launches++;
+    if (Dh0) {
+        reduce_partials_kernel<<<1, 256, 0, c->st>>>(c->partials, c->red_blocks, nh + 1, c->red);
+        c->launches++;
+    }
+}
+
+void enqueue_concs_any(lfts_ctx *c, double *Dh0, int nh, const HistPtrs &hist)
+{
+    if (c->prec == LFTS_FP64)
+        enqueue_concs<double>(c, Dh0, nh, hist);
+    else
+        enqueue_concs<float>(c, Dh0, nh, hist);
+}
+
+// One chain with CUDA events around every contour-step kernel; returns the
+// mean duration of the yz-plane (STEP) and x-pencil (CONV) launches and the
+// whole chain (first launch to Q).
+template <typename T>
+int profile_chain(lfts_ctx *c, double *ms_plane, double *ms_pencil, double *ms_chain)
+{
+    const int n = c->N - 1;
+    std::vector<cudaEvent_t> ev(4 * n + 2);
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    T *q = static_cast<T *>(c->q);
+    const long long M = c->M;
+    PlaneArgs<T> a = plane_args<T>(c);
+    a.qout = q;
+    CK(cudaEventRecord(ev[4 * n], c->st));
+    launch_plane<T>(c, PLANE_INIT_W, a, 2);
+    PencilArgs<T> pa = pencil_args<T>(c);
+    a.h = q;
+    for (int i = 1; i < c->N; i++) {
+        const int j = i - 1;
+        CK(cudaEventRecord(ev[4 * j], c->st));
+        launch_pencil<T>(c, PENCIL_CONV, pa, 2);
+        CK(cudaEventRecord(ev[4 * j + 1], c->st));
+        a.qout = q + (long long)i * 2 * M;
+        a.hsel0 = hsel_chain0(c, i);
+        a.hsel1 = hsel_chain1(c, i);
+        CK(cudaEventRecord(ev[4 * j + 2], c->st));
+        launch_plane<T>(c, i + 1 < c->N ? PLANE_STEP : PLANE_LAST, a, 2);
+        CK(cudaEventRecord(ev[4 * j + 3], c->st));
+    }
+    q_finalize_kernel<<<1, 256, 0, c->st>>>(c->qpart, c->mx, M, c->Qd);
+    c->launches++;
+    CK(cudaEventRecord(ev[4 * n + 1], c->st));
+    CK(cudaEventSynchronize(ev[4 * n + 1]));
+    double pl = 0.0, pe = 0.0;
+    int npl = 0;
+    for (int j = 0; j < n; j++) {
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, ev[4 * j], ev[4 * j + 1]));
+        pe += t;
+        if (j + 1 < n) {
+            CK(cudaEventElapsedTime(&t, ev[4 * j + 2], ev[4 * j + 3]));
+            pl += t;
+            npl++;
+        }
+    }
+    float tc = 0.f;
+    CK(cudaEventElapsedTime(&tc, ev[4 * n], ev[4 * n + 1]));
+    for (auto &e : ev) cudaEventDestroy(e);
+    *ms_pencil = pe / n;
+    *ms_plane = npl ? pl / npl : 0.0;
+    *ms_chain = tc;
+    return LFTS_OK;
+}
+
+int calc_concs_sync(lfts_ctx *c, double *lnQ)
+{
+    HistPtrs none{};
+    enqueue_concs_any(c, nullptr, 0, none);
+    CK(cudaGetLastError());
+    if (lnQ) {
+        CK(cudaMemcpyAsync(c->red_host, c->Qd, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        *lnQ = c->red_host[1];
+    }
+    c->have_concs = true;
+    return LFTS_OK;
+}
+
+// anderson::mix (src/anderson.cc:24-93) with the history kept as a ring of
+// physical buffers addressed through the reference's logical slot numbers.
+int anderson_mix(lfts_ctx *c, int maxIter, double errTol, int *k_out)
+{
+    const int nhMax = kMaxHist;
+    const long long M = c->M;
+    double err = 1.0;
+    int k;
+    for (k = 1; k < maxIter && err > errTol; k++) {
+        const int nh = (k < nhMax + 1) ? k - 1 : nhMax;
+        HistPtrs Dhp{}, whp{};
+        for (int m = 1; m <= nh; m++) {
+            Dhp.p[m - 1] = c->Dh[c->phys[m]];
+            whp.p[m - 1] = c->wh[c->phys[m]];
+        }
+        double *Dh0 = c->Dh[c->cur];
+        enqueue_concs_any(c, Dh0, nh, Dhp);
+        CK(cudaMemcpyAsync(c->red_host, c->red, (nh + 1) * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        const double S1 = c->red_host[0];
+        err = std::pow(S1 / (double)M, 0.5);
+        const double lambda = 1.0 - std::pow(0.9, double(k));
+        for (int m = 0; m <= nh; m++) c->DD[0][m] = c->red_host[m];
+
+        Coefs C{};
+        int simple = 1;
+        if (k >= 2) {
+            simple = 0;
+            std::vector<double> U((size_t)nh * nh), V(nh);
+            for (int m = 1; m <= nh; m++) {
+                V[m - 1] = c->DD[0][0] - c->DD[0][m];
+                for (int n = 1; n <= m; n++) {
+                    const double u = c->DD[0][0] - c->DD[0][m] - c->DD[0][n] + c->DD[n][m];
+                    U[(m - 1) * nh + n - 1] = u;
+                    U[(n - 1) * nh + m - 1] = u;
+                }
+            }
+            if (!lu_solve(U, V, C.c, nh)) {
+                g_last_error = "Anderson least-squares matrix is singular";
+                return LFTS_ERR_SINGULAR;
+            }
+        }
+        anderson_update_kernel<<<stream_grid(c), 256, 0, c->st>>>(c->w + M, c->wh[c->cur], Dh0, M, lambda, nh,
+                                                                  simple, Dhp, whp, C);
+        c->launches++;
+        CK(cudaGetLastError());
+
+        // the current field and deviation become history slot n (src/anderson.cc:82-89)
+        const int n = 1 + (k - 1) % nhMax;
+        const int evicted = c->phys[n];
+        c->phys[n] = c->cur;
+        c->cur = evicted;
+        c->DD[n][n] = c->DD[0][0];
+        for (int m = 1; m < n; m++) c->DD[m][n] = c->DD[0][m];
+        for (int m = n + 1; m <= nh; m++) c->DD[n][m] = c->DD[0][m];
+        c->mix_iters++;
+    }
+    c->mix_calls++;
+    if (k_out) *k_out = k;
+    c->have_concs = true;
+    return LFTS_OK;
+}
+
+// ---- structure function -------------------------------------------------------
+int sk_sample(lfts_ctx *c)
+{
+    PlaneArgs<double> a{};
+    a.src64 = c->w;  // W-
+    a.src_stride = 0;
+    a.spec = static_cast<cpx<double> *>(c->skspec);
+    const bool fp64 = c->prec == LFTS_FP64;
+    a.twy = static_cast<const cpx<double> *>(fp64 ? c->tw[1] : c->sktw[1]);
+    a.twz = static_cast<const cpx<double> *>(fp64 ? c->tw[2] : c->sktw[2]);
+    a.Nd = (double)c->N;
+    c->pl64.fn[PLANE_INIT_Q]<<<dim3(c->mx, 1), c->pl64.nt, c->pl64.smem, c->st>>>(a);
+    PencilArgs<double> pa{};
+    pa.spec = a.spec;
+    pa.twx = static_cast<const cpx<double> *>(fp64 ? c->tw[0] : c->sktw[0]);
+    pa.S = c->S;
+    pa.ncol = c->my * c->KZ;
+    pa.KZ = c->KZ;
+    const int ncol = pa.ncol;
+    c->pe64.fn[PENCIL_POWER]<<<dim3((ncol + c->pe64.cw - 1) / c->pe64.cw, 1), c->pe64.nt, c->pe64.smem, c->st>>>(pa);
+    c->launches += 2;
+    CK(cudaGetLastError());
+    c->nsamples++;
+    return LFTS_OK;
+}
+
+// |K| of every half-spectrum index (src/strFunc.cc:80-103) and bin tables
+int sk_prepare_bins(lfts_ctx *c, double dK)
+{
+    const int m[3] = {c->mx, c->my, c->mz};
+    const double *L = c->p.L;
+    const long long Mk = c->Mk;
+    std::vector<double> K(Mk);
+    std::vector<int> wt(Mk, 2), P(Mk);
+    for (int k0 = -(m[0] - 1) / 2; k0 <= m[0] / 2; k0++) {
+        const int K0 = (k0 < 0) ? (k0 + m[0]) : k0;
+        const double kx_sq = k0 * k0 / (L[0] * L[0]);
+        for (int k1 = -(m[1] - 1) / 2; k1 <= m[1] / 2; k1++) {
+            const int K1 = (k1 < 0) ? (k1 + m[1]) : k1;
+            const double ky_sq = k1 * k1 / (L[1] * L[1]);
+            for (int k2 = 0; k2 <= m[2] / 2; k2++) {
+                const double kz_sq = k2 * k2 / (L[2] * L[2]);
+                const long long k = k2 + (long long)(m[2] / 2 + 1) * (K1 + (long long)m[1] * K0);
+                K[k] = kTwoPi * std::pow(kx_sq + ky_sq + kz_sq, 0.5);
+                if (k2 == 0 || k2 == m[2] / 2) wt[k] = 1;
+            }
+        }
+    }
+    std::iota(P.begin(), P.end(), 0);
+    std::stable_sort(P.begin(), P.end(), [&](int i, int j) { return K[i] < K[j]; });
+    std::vector<int> bins;
+    c->sk_K.clear();
+    bins.push_back(0);
+    for (long long k = 0; k < Mk; k++) {
+        if (k == Mk - 1 || std::fabs(K[P[k + 1]] - K[P[k]]) > dK) {
+            bins.push_back((int)k + 1);
+            c->sk_K.push_back(K[P[k]]);
+        }
+    }
+    cudaFree(c->sk_order);
+    cudaFree(c->sk_wt);
+    cudaFree(c->sk_bins);
+    cudaFree(c->sk_out);
+    c->sk_nbins = (int)bins.size() - 1;
+    CK(cudaMalloc(&c->sk_order, sizeof(int) * Mk));
+    CK(cudaMalloc(&c->sk_wt, sizeof(int) * Mk));
+    CK(cudaMalloc(&c->sk_bins, sizeof(int) * bins.size()));
+    CK(cudaMalloc(&c->sk_out, sizeof(double) * c->sk_nbins));
+    CK(cudaMemcpy(c->sk_order, P.data(), sizeof(int) * Mk, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->sk_wt, wt.data(), sizeof(int) * Mk, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->sk_bins, bins.data(), sizeof(int) * bins.size(), cudaMemcpyHostToDevice));
+    c->sk_dK = dK;
+    return LFTS_OK;
+}
+
+int ctx_alloc(lfts_ctx *c)
+{
+    const long long M = c->M;
+    CK(cudaMalloc(&c->w, sizeof(double) * 4 * M));
+    CK(cudaMemset(c->w, 0, sizeof(double) * 4 * M));
+    CK(cudaMalloc(&c->q, c->tsize * 2 * M * (size_t)c->N));
+    CK(cudaMalloc(&c->spec, c->tsize * 2 * 2 * (size_t)c->mx * c->my * c->KZ));
+    CK(cudaMalloc(&c->qpart, sizeof(double) * c->mx));
+    CK(cudaMalloc(&c->Qd, sizeof(double) * 2));
+    CK(cudaMalloc(&c->partials, sizeof(double) * kRedWidth * c->red_blocks));
+    CK(cudaMalloc(&c->red, sizeof(double) * kRedWidth));
+    CK(cudaMallocHost(&c->red_host, sizeof(double) * kRedWidth));
+    for (int i = 0; i < 2; i++) {
+        CK(cudaMalloc(&c->eta[i], sizeof(double) * M));
+        CK(cudaMemset(c->eta[i], 0, sizeof(double) * M));
+    }
+    for (int i = 0; i < kRedWidth; i++) {
+        CK(cudaMalloc(&c->Dh[i], sizeof(double) * M));
+        CK(cudaMalloc(&c->wh[i], sizeof(double) * M));
+        CK(cudaMemset(c->Dh[i], 0, sizeof(double) * M));
+        CK(cudaMemset(c->wh[i], 0, sizeof(double) * M));
+    }
+    // logical slots 1..10 -> buffers 1..10, buffer 0 is the first current one
+    for (int i = 0; i < kRedWidth; i++) c->phys[i] = i;
+    c->cur = 0;
+    CK(cudaMalloc(&c->S, sizeof(double) * c->Mk));
+    CK(cudaMemset(c->S, 0, sizeof(double) * c->Mk));
+    if (c->prec == LFTS_FP64) {
+        c->skspec = c->spec;
+    } else {
+        CK(cudaMalloc(&c->skspec, sizeof(cpx<double>) * (size_t)c->Mk));
+        c->sk_own_spec = true;
+    }
+    return LFTS_OK;
+}
+
+void ctx_free(lfts_ctx *c)
+{
+    if (c->st) cudaStreamSynchronize(c->st);
+    cudaFree(c->w);
+    cudaFree(c->q);
+    cudaFree(c->spec);
+    for (int d = 0; d < 3; d++) {
+        cudaFree(c->tw[d]);
+        cudaFree(c->gtab[d]);
+        cudaFree(c->sktw[d]);
+    }
+    cudaFree(c->qpart);
+    cudaFree(c->Qd);
+    cudaFree(c->partials);
+    cudaFree(c->red);
+    if (c->red_host) cudaFreeHost(c->red_host);
+    for (int i = 0; i < 2; i++) cudaFree(c->eta[i]);
+    for (int i = 0; i < kRedWidth; i++) {
+        cudaFree(c->Dh[i]);
+        cudaFree(c->wh[i]);
+    }
+    cudaFree(c->S);
+    if (c->sk_own_spec) cudaFree(c->skspec);
+    cudaFree(c->sk_order);
+    cudaFree(c->sk_wt);
+    cudaFree(c->sk_bins);
+    cudaFree(c->sk_out);
+    cudaFree(c->sf_buf);
+    if (c->st) cudaStreamDestroy(c->st);
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+namespace {
+template <typename T>
+int step_fwd_impl(lfts_ctx *c, const double *q_in, double *q_out, const double *h, int i)
+{
+    const long long M = c->M;
+    double *dq = static_cast<double *>(c->sf_buf);
+    double *dout = dq + 2 * M, *dh = dq + 4 * M;
+    T *tq = reinterpret_cast<T *>(dh + 2 * M);  // T copies when T != double
+    T *th = tq + 2 * M;
+    T *tout = th + 2 * M;
+    CK(cudaMemcpyAsync(dq, q_in, sizeof(double) * 2 * M, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(dh, h, sizeof(double) * 2 * M, cudaMemcpyHostToDevice, c->st));
+    const T *src = reinterpret_cast<const T *>(dq), *hh = reinterpret_cast<const T *>(dh);
+    T *dst = reinterpret_cast<T *>(dout);
+    if (sizeof(T) != sizeof(double)) {
+        convert_kernel<double, T><<<stream_grid(c), 256, 0, c->st>>>(dq, tq, 2 * M);
+        convert_kernel<double, T><<<stream_grid(c), 256, 0, c->st>>>(dh, th, 2 * M);
+        c->launches += 2;
+        src = tq;
+        hh = th;
+        dst = tout;
+    }
+    PlaneArgs<T> a = plane_args<T>(c);
+    a.src = src;
+    a.src_stride = M;
+    launch_plane<T>(c, PLANE_INIT_Q, a, 2);
+    launch_pencil<T>(c, PENCIL_CONV, pencil_args<T>(c), 2);
+    a.qout = dst;
+    a.h = hh;
+    a.hsel0 = hsel_chain0(c, i);
+    a.hsel1 = hsel_chain1(c, i);
+    launch_plane<T>(c, PLANE_LAST, a, 2);
+    if (sizeof(T) != sizeof(double)) {
+        convert_kernel<T, double><<<stream_grid(c), 256, 0, c->st>>>(tout, dout, 2 * M);
+        c->launches++;
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(q_out, dout, sizeof(double) * 2 * M, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return LFTS_OK;
+}
+
+}  // namespace
+
+}  // namespace
+
+// =============================================================================
+extern "C" {
+
+const char *lfts_version(void) { return "lfts_b200 0.1 (sm_100a)"; }
+
+const char *lfts_status_string(int s)
+{
+    switch (s) {
+        case LFTS_OK: return "ok";
+        case LFTS_ERR_ARG: return "invalid argument";
+        case LFTS_ERR_UNSUPPORTED: return "mesh size not supported by the FFT kernels";
+        case LFTS_ERR_CUDA: return "CUDA error";
+        case LFTS_ERR_NOMEM: return "device allocation failed";
+        case LFTS_ERR_SINGULAR: return "Anderson least-squares matrix singular";
+        case LFTS_ERR_STATE: return "call out of order";
+        case LFTS_ERR_NOTCONV: return "iteration cap reached";
+        default: return "unknown status";
+    }
+}
+
+const char *lfts_last_error_string(void) { return g_last_error.c_str(); }
+
+int lfts_mesh_supported(int n) { return fft_length_supported(n) ? 1 : 0; }
+
+int lfts_create(const lfts_params *p, int precision, int device, lfts_ctx **out)
+{
+    if (!p || !out) return LFTS_ERR_ARG;
+    *out = nullptr;
+    if (p->N < 2 || p->NA < 0 || p->NA > p->N || p->C <= 0.0 || p->XbN == 0.0) return LFTS_ERR_ARG;
+    if (precision != LFTS_FP64 && precision != LFTS_FP32_MIXED) return LFTS_ERR_ARG;
+    for (int d = 0; d < 3; d++)
+        if (p->m[d] < 1 || !(p->L[d] > 0.0)) return LFTS_ERR_ARG;
+    if (!fft_length_supported(p->m[0]) || !plane_pair_supported(p->m[1], p->m[2]) || (p->m[1] % 2)) {
+        g_last_error = "mesh not supported: each dimension must be one of the compiled FFT lengths";
+        return LFTS_ERR_UNSUPPORTED;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        g_last_error = "no CUDA device";
+        return LFTS_ERR_CUDA;
+    }
+    DeviceGuard g(device);
+    lfts_ctx *c = new lfts_ctx;
+    c->p = *p;
+    c->prec = precision;
+    c->dev = device;
+    c->N = p->N;
+    c->NA = p->NA;
+    c->NB = p->N - p->NA;
+    c->mx = p->m[0];
+    c->my = p->m[1];
+    c->mz = p->m[2];
+    c->KZ = c->mz / 2 + 1;
+    c->M = (long long)c->mx * c->my * c->mz;
+    c->Mk = (long long)c->mx * c->my * c->KZ;
+    c->tsize = precision == LFTS_FP64 ? sizeof(double) : sizeof(float);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->sms = prop.multiProcessorCount;
+    c->red_blocks = c->sms * 4;
+    int rc = LFTS_OK;
+    auto fail = [&](int code) {
+        ctx_free(c);
+        delete c;
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) return fail(LFTS_ERR_CUDA);
+    if (!plane_kernels(c->my, c->mz, &c->pl64) || !pencil_kernels(c->mx, &c->pe64)) return fail(LFTS_ERR_UNSUPPORTED);
+    if ((rc = set_smem_attrs(c->pl64, c->pe64))) return fail(rc);
+    if (precision == LFTS_FP32_MIXED) {
+        if (!plane_kernels(c->my, c->mz, &c->pl32) || !pencil_kernels(c->mx, &c->pe32)) return fail(LFTS_ERR_UNSUPPORTED);
+        if ((rc = set_smem_attrs(c->pl32, c->pe32))) return fail(rc);
+    }
+    if ((rc = ctx_alloc(c))) return fail(rc == LFTS_ERR_CUDA ? LFTS_ERR_NOMEM : rc);
+    if (precision == LFTS_FP64)
+        rc = upload_tables<double>(c, c->tw, c->gtab);
+    else {
+        rc = upload_tables<float>(c, c->tw, c->gtab);
+        if (!rc) rc = upload_tables<double>(c, c->sktw, nullptr);
+    }
+    if (rc) return fail(rc);
+    *out = c;
+    return LFTS_OK;
+}
+
+int lfts_destroy(lfts_ctx *c)
+{
+    if (!c) return LFTS_OK;
+    DeviceGuard g(c->dev);
+    ctx_free(c);
+    delete c;
+    return LFTS_OK;
+}
+
+int lfts_device_bytes(const lfts_ctx *c, size_t *bytes)
+{
+    if (!c || !bytes) return LFTS_ERR_ARG;
+    const size_t M = c->M;
+    size_t b = 4 * M * 8 + c->tsize * 2 * M * c->N + c->tsize * 4 * (size_t)c->mx * c->my * c->KZ;
+    b += 2 * M * 8 + 2 * kRedWidth * M * 8 + c->Mk * 8;
+    if (c->sk_own_spec) b += c->Mk * 16;
+    *bytes = b;
+    return LFTS_OK;
+}
+
+int lfts_set_fields(lfts_ctx *c, const double *w_host)
+{
+    if (!c || !w_host) return LFTS_ERR_ARG;
+    DeviceGuard g(c->dev);
+    CK(cudaMemcpyAsync(c->w, w_host, sizeof(double) * 2 * c->M, cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->fields_set = true;
+    return LFTS_OK;
+}
+
+int lfts_get_fields(lfts_ctx *c, double *w_host)
+{
+    if (!c || !w_host) return LFTS_ERR_ARG;
+    DeviceGuard g(c->dev);
+    CK(cudaMemcpyAsync(w_host, c->w, sizeof(double) * 4 * c->M, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return LFTS_OK;
+}
+
+int lfts_fields_device(lfts_ctx *c, double **w_dev)
+{
+    if (!c || !w_dev) return LFTS_ERR_ARG;
+    *w_dev = c->w;
+    c->fields_set = true;  // the caller may fill the array directly
+    return LFTS_OK;
+}
+
+int lfts_calc_concs(lfts_ctx *c, double *lnQ)
+{
+    if (!c) return LFTS_ERR_ARG;
+    if (!c->fields_set) return LFTS_ERR_STATE;
+    DeviceGuard g(c->dev);
+    return calc_concs_sync(c, lnQ);
+}
+
+int lfts_anderson_mix(lfts_ctx *c, int maxIter, double errTol, int *k_out)
+{
+    if (!c) return LFTS_ERR_ARG;
+    if (!c->fields_set) return LFTS_ERR_STATE;
+    DeviceGuard g(c->dev);
+    return anderson_mix(c, maxIter, errTol, k_out);
+}
+
+int lfts_langevin_init(lfts_ctx *c, const double *noise_prev_host)
+{
+    if (!c || !noise_prev_host) return LFTS_ERR_ARG;
+    DeviceGuard g(c->dev);
+    c->eta_prev = 0;
+    CK(cudaMemcpyAsync(c->eta[0], noise_prev_host, sizeof(double) * c->M, cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->eta_set = true;
+    return LFTS_OK;
+}
+
+static int langevin_device(lfts_ctx *c, const double *eta_new_dev)
+{
+    const int nb = 1 - c->eta_prev;
+    if (eta_new_dev != c->eta[nb])
+        CK(cudaMemcpyAsync(c->eta[nb], eta_new_dev, sizeof(double) * c->M, cudaMemcpyDeviceToDevice, c->st));
+    langevin_kernel<<<stream_grid(c), 256, 0, c->st>>>(c->w, c->M, c->eta[c->eta_prev], c->eta[nb], c->p.XbN,
+                                                       c->p.dt);
+    c->launches++;
+    CK(cudaGetLastError());
+    c->eta_prev = nb;  // the new noise is the next step's previous noise (src/langevin.cc:34-36)
+    return LFTS_OK;
+}
+
+int lfts_langevin_step(lfts_ctx *c, const double *noise_new_host)
+{
+    if (!c || !noise_new_host) return LFTS_ERR_ARG;
+    if (!c->fields_set || !c->eta_set || !c->have_concs) return LFTS_ERR_STATE;
+    DeviceGuard g(c->dev);
+    const int nb = 1 - c->eta_prev;
+    CK(cudaMemcpyAsync(c->eta[nb], noise_new_host, sizeof(double) * c->M, cudaMemcpyHostToDevice, c->st));
+    int rc = langevin_device(c, c->eta[nb]);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->st));
+    return LFTS_OK;
+}
+
+int lfts_langevin_step_device(lfts_ctx *c, const double *noise_new_dev)
+{
+    if (!c || !noise_new_dev) return LFTS_ERR_ARG;
+    if (!c->fields_set || !c->eta_set || !c->have_concs) return LFTS_ERR_STATE;
+    DeviceGuard g(c->dev);
+    return langevin_device(c, noise_new_dev);
+}
+
+int lfts_langevin_full_step(lfts_ctx *c, const double *noise_new_dev, int maxIter, double errTol, int *k_out,
+                            double *lnQ)
+{
+    if (!c || !noise_new_dev) return LFTS_ERR_ARG;
+    if (!c->fields_set || !c->eta_set || !c->have_concs) return LFTS_ERR_STATE;
+    DeviceGuard g(c->dev);
+    int rc = langevin_device(c, noise_new_dev);
+    if (!rc) rc = anderson_mix(c, maxIter, errTol, k_out);
+    if (!rc) rc = calc_concs_sync(c, lnQ);
+    return rc;
+}
+
+int lfts_sk_sample(lfts_ctx *c)
+{
+    if (!c) return LFTS_ERR_ARG;
+    if (!c->fields_set) return LFTS_ERR_STATE;
+    DeviceGuard g(c->dev);
+    int rc = sk_sample(c);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->st));
+    return LFTS_OK;
+}
+
+int lfts_sk_get(lfts_ctx *c, double *S_host, int *nsamples)
+{
+    if (!c) return LFTS_ERR_ARG;
+    DeviceGuard g(c->dev);
+    if (S_host) {
+        CK(cudaMemcpyAsync(S_host, c->S, sizeof(double) * c->Mk, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+    }
+    if (nsamples) *nsamples = c->nsamples;
+    return LFTS_OK;
+}
+
+int lfts_sk_reset(lfts_ctx *c)
+{
+    if (!c) return LFTS_ERR_ARG;
+    DeviceGuard g(c->dev);
+    CK(cudaMemsetAsync(c->S, 0, sizeof(double) * c->Mk, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->nsamples = 0;
+    return LFTS_OK;
+}
+
+int lfts_sk_bin(lfts_ctx *c, double dK, double *K_out, double *S_out, int *nbins)
+{
+    if (!c || !K_out || !S_out || !nbins || !(dK >= 0.0)) return LFTS_ERR_ARG;
+    if (c->nsamples < 1) return LFTS_ERR_STATE;
+    DeviceGuard g(c->dev);
+    if (dK != c->sk_dK) {
+        int rc = sk_prepare_bins(c, dK);
+        if (rc) return rc;
+    }
+    // coeff_ = CV/(chi_b^2 M^2) (src/strFunc.cc:21), with CV = C*V
+    const double V = c->p.L[0] * c->p.L[1] * c->p.L[2];
+    const double CV = c->p.C * V;
+    const double M = (double)c->M;
+    const double coeff = CV / (c->p.XbN * c->p.XbN * M * M);
+    sk_bin_kernel<<<(c->sk_nbins + 127) / 128, 128, 0, c->st>>>(c->S, c->sk_order, c->sk_wt, c->sk_bins,
+                                                               c->sk_nbins, coeff / c->nsamples, 0.5 / c->p.XbN,
+                                                               c->sk_out);
+    c->launches++;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(S_out, c->sk_out, sizeof(double) * c->sk_nbins, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    std::memcpy(K_out, c->sk_K.data(), sizeof(double) * c->sk_nbins);
+    *nbins = c->sk_nbins;
+    return LFTS_OK;
+}
+
+int lfts_get_H(lfts_ctx *c, double *H)
+{
+    if (!c || !H) return LFTS_ERR_ARG;
+    if (!c->fields_set) return LFTS_ERR_STATE;
+    DeviceGuard g(c->dev);
+    double lnQ = 0.0;
+    int rc = calc_concs_sync(c, &lnQ);
+    if (rc) return rc;
+    h_sums_kernel<<<stream_grid(c), kRedThreads, 0, c->st>>>(c->w, c->M, c->partials);
+    reduce_partials_kernel<<<1, 256, 0, c->st>>>(c->partials, c->red_blocks, 2, c->red);
+    c->launches += 2;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(c->red_host, c->red, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    const double wp_sum = c->red_host[0], wm2_sum = c->red_host[1];
+    *H = -lnQ + (wm2_sum / c->p.XbN - wp_sum) / (double)c->M;
+    return LFTS_OK;
+}
+
+int lfts_step_fwd(lfts_ctx *c, const double *q_in, double *q_out, const double *h, int i)
+{
+    if (!c || !q_in || !q_out || !h || i < 1 || i >= c->N) return LFTS_ERR_ARG;
+    DeviceGuard g(c->dev);
+    if (!c->sf_buf) CK(cudaMalloc(&c->sf_buf, sizeof(double) * 6 * c->M + c->tsize * 6 * c->M));
+    if (c->prec == LFTS_FP64) return step_fwd_impl<double>(c, q_in, q_out, h, i);
+    return step_fwd_impl<float>(c, q_in, q_out, h, i);
+}
+
+int lfts_g_lookup(lfts_ctx *c, double *g_host)
+{
+    if (!c || !g_host) return LFTS_ERR_ARG;
+    // the factorised weights the kernels multiply by, expanded to the Mk layout
+    const int m[3] = {c->mx, c->my, c->mz};
+    std::vector<double> g[3];
+    const int n[3] = {c->mx, c->my, c->KZ};
+    for (int d = 0; d < 3; d++) {
+        g[d].resize(n[d]);
+        for (int K = 0; K < n[d]; K++) {
+            const int k = (d == 2) ? K : signed_k(K, m[d]);
+            const double ksq = (double)k * k / (c->p.L[d] * c->p.L[d]);
+            double v = std::exp(-kTwoPi * kTwoPi * ksq / (6.0 * c->N));
+            if (d == 2) v /= (double)c->M;
+            g[d][K] = (c->prec == LFTS_FP64) ? v : (double)(float)v;
+        }
+    }
+    for (int a = 0; a < c->mx; a++)
+        for (int b = 0; b < c->my; b++)
+            for (int k = 0; k < c->KZ; k++)
+                g_host[((long long)a * c->my + b) * c->KZ + k] = g[0][a] * g[1][b] * g[2][k];
+    return LFTS_OK;
+}
+
+void *lfts_stream(lfts_ctx *c) { return c ? (void *)c->st : nullptr; }
+
+int lfts_profile_chain(lfts_ctx *c, double *ms_plane, double *ms_pencil, double *ms_chain)
+{
+    if (!c || !ms_plane || !ms_pencil || !ms_chain) return LFTS_ERR_ARG;
+    if (!c->fields_set) return LFTS_ERR_STATE;
+    DeviceGuard g(c->dev);
+    CK(cudaStreamSynchronize(c->st));
+    if (c->prec == LFTS_FP64) return profile_chain<double>(c, ms_plane, ms_pencil, ms_chain);
+    return profile_chain<float>(c, ms_plane, ms_pencil, ms_chain);
+}
+
+long long lfts_kernel_launches(const lfts_ctx *c) { return c ? c->launches : 0; }
+
+int lfts_anderson_stats(const lfts_ctx *c, long long *calls, long long *iterations)
+{
+    if (!c) return LFTS_ERR_ARG;
+    if (calls) *calls = c->mix_calls;
+    if (iterations) *iterations = c->mix_iters;
+    return LFTS_OK;
+}
+
+int lfts_get_propagators(lfts_ctx *c, double *q_host)
+{
+    if (!c || !q_host) return LFTS_ERR_ARG;
+    DeviceGuard g(c->dev);
+    const long long n = 2 * c->M * (long long)c->N;
+    std::memset(q_host, 0, sizeof(double) * 2 * c->M);
+    if (c->prec == LFTS_FP64) {
+        CK(cudaMemcpyAsync(q_host + 2 * c->M, c->q, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+    } else {
+        std::vector<float> tmp(n);
+        CK(cudaMemcpyAsync(tmp.data(), c->q, sizeof(float) * n, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        for (long long i = 0; i < n; i++) q_host[2 * c->M + i] = tmp[i];
+    }
+    return LFTS_OK;
+}
+
+}  // extern "C"

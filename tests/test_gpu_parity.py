@@ -1,0 +1,202 @@
+"""Parity of the CUDA path (called through the C ABI) with the reference:
+golden fixtures made from the reference's own classes, the C oracle live at
+larger meshes, and size-independent identities at the full 128^3, N=64 size.
+
+Tolerances: FP64 path 1e-10 relative (the bar the reference is held to);
+FP32-mixed path 1e-5 on phi."""
+import numpy as np
+import pytest
+
+from conftest import golden, rel_err
+from helpers import parse_header, ref_input40_fields
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+FP32_PHI_TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def lfts(native_lib):
+    import lfts_cpu_b200
+    return lfts_cpu_b200
+
+
+def make_system(lfts, g, precision=0):
+    m = tuple(int(v) for v in g["m"])
+    L = tuple(float(v) for v in g["L"])
+    NA, NB = int(g["NA"]), int(g["NB"])
+    return lfts.System(NA + NB, NA, 12.0, 50.0, 0.5, m, L, precision=precision), int(np.prod(m))
+
+
+@pytest.mark.parametrize("name", ["comp_16", "comp_12x24x16", "comp_8x12x20"])
+def test_calc_concs_fp64_matches_reference(lfts, name):
+    g = golden(name)
+    s, M = make_system(lfts, g)
+    s.set_fields(g["w_in"])
+    lnQ = s.calc_concs()
+    w = s.get_fields()
+    assert abs(lnQ - float(g["lnQ"])) < FP64_TOL * max(1.0, abs(float(g["lnQ"])))
+    assert rel_err(w[2 * M:], g["phi"]) < FP64_TOL
+    assert np.array_equal(w[: 2 * M], g["w_in"])
+
+
+@pytest.mark.parametrize("name", ["comp_16", "comp_12x24x16", "comp_8x12x20"])
+def test_step_fwd_fp64_matches_reference(lfts, name):
+    g = golden(name)
+    s, M = make_system(lfts, g)
+    for j, i in enumerate(g["steps"]):
+        out = s.step_fwd(g["q_in"], g["h"], int(i))
+        assert rel_err(out, g["q_out"][j]) < FP64_TOL
+
+
+@pytest.mark.parametrize("name", ["comp_16", "comp_8x12x20"])
+def test_g_lookup_matches_reference(lfts, name):
+    g = golden(name)
+    s, M = make_system(lfts, g)
+    assert rel_err(s.g_lookup(), g["g"]) < 1e-14
+
+
+@pytest.mark.parametrize("name", ["comp_16", "comp_12x24x16", "comp_8x12x20"])
+def test_anderson_mix_fp64_matches_reference(lfts, name):
+    g = golden(name)
+    s, M = make_system(lfts, g)
+    s.set_fields(g["w_in"])
+    K = s.mix()
+    w = s.get_fields()
+    assert K == int(g["mix_K"])
+    assert rel_err(w[M:2 * M], g["mix_w"][M:2 * M]) < 1e-9
+    assert rel_err(w[2 * M:], g["mix_w"][2 * M:]) < 1e-9
+
+
+@pytest.mark.parametrize("name", ["comp_16", "comp_12x24x16"])
+def test_calc_concs_fp32_mixed_error_bound(lfts, name):
+    g = golden(name)
+    s, M = make_system(lfts, g, precision=lfts.LFTS_FP32_MIXED)
+    s.set_fields(g["w_in"])
+    lnQ = s.calc_concs()
+    w = s.get_fields()
+    assert abs(lnQ - float(g["lnQ"])) < 1e-5
+    assert rel_err(w[2 * M:], g["phi"]) < FP32_PHI_TOL
+
+
+# Runs whose Anderson iteration count flips under 1e-15 input perturbations of
+# the reference itself (tests/test_oracle_cpu.py::test_lamellar_mix_is_roundoff_sensitive);
+# they are held to the saddle-point tolerance instead of 1e-10.
+ROUNDOFF_SENSITIVE = {"traj_lam24"}
+
+
+def check_sensitive_trajectory(s, g, rng, M):
+    w0 = s.get_fields()
+    # converged to the same saddle point within the mixing tolerance (1e-4)
+    assert np.max(np.abs(w0[M:2 * M] - g["w0"][M:2 * M])) < 1e-3
+    assert np.sqrt(np.mean((w0[3 * M:] - 1.0) ** 2)) < 2e-4
+    lnQs = []
+    n = int(g["n_eq"]) + int(g["n_st"])
+    for it in range(n):
+        s.langevin_step(rng.normal(M))
+        s.mix()
+        lnQs.append(s.calc_concs())
+    assert np.max(np.abs(np.array(lnQs) - g["lnQ"])) < 1e-4
+    w = s.get_fields()
+    assert np.sqrt(np.mean((w[3 * M:] - 1.0) ** 2)) < 2e-4
+    assert np.max(np.abs(w[:M] - g["w_end"][:M])) < 1e-3 * np.max(np.abs(g["w_end"][:M]))
+
+
+@pytest.mark.parametrize("name", ["traj_valgrind16", "traj_16", "traj_lam24"])
+def test_trajectory_fp64_matches_reference(lfts, name):
+    """Whole reference runs replayed on the GPU with the same noise stream:
+    initial mix, Langevin steps (K sequence equal, ln Q, fields), S(k), H."""
+    g = golden(name)
+    hdr = parse_header([str(s) for s in g["header"]])
+    N, NA, m, L = hdr["N"], hdr["NA"], hdr["m"], hdr["L"]
+    M = int(np.prod(m))
+    XbN, sigma = float(g["XbN"]), float(g["sigma"])
+    s = lfts.System(N, NA, XbN, hdr["C"], hdr["dt"], m, L)
+    rng = lfts.Rng(123456789, sigma)
+    s.langevin_init(rng.normal(M))
+    w2 = lfts.lamellar_field(XbN, m) if hdr["loadType"] == 2 else rng.random_field(XbN, M)
+    s.set_fields(w2)
+    s.mix()
+    if name in ROUNDOFF_SENSITIVE:
+        return check_sensitive_trajectory(s, g, rng, M)
+    assert rel_err(s.get_fields(), g["w0"]) < 1e-9
+    Ks, lnQs = [], []
+    n_eq, n_st, every = int(g["n_eq"]), int(g["n_st"]), int(g["sample_every"])
+    for it in range(n_eq + n_st):
+        s.langevin_step(rng.normal(M))
+        Ks.append(s.mix())
+        lnQs.append(s.calc_concs())
+        if it >= n_eq and (it - n_eq + 1) % every == 0:
+            s.sk_sample()
+    assert Ks == list(g["K"])
+    assert np.max(np.abs(np.array(lnQs) - g["lnQ"])) < FP64_TOL
+    w = s.get_fields()
+    assert rel_err(w, g["w_end"]) < 1e-8
+    S, ns = s.sk_get()
+    assert ns == int(g["nsamples"])
+    if ns:
+        assert rel_err(S, g["S"]) < 1e-8
+        K, Sb = s.sk_bin(1e-5)
+        ref = np.array([[float(v) for v in ln.split("\t")] for ln in str(g["struct_text"]).strip().split("\n")])
+        assert len(K) == len(ref)
+        assert np.max(np.abs(K - ref[:, 0])) < 1e-8
+        assert np.max(np.abs(Sb - ref[:, 1])) < 1e-6
+    assert abs(s.get_H() - float(g["H"])) < FP64_TOL * 10
+
+
+def test_reference_input40_fixture(lfts):
+    g = golden("ref_input40")
+    hdr, fields = ref_input40_fields()
+    p = parse_header(hdr)
+    M = int(np.prod(p["m"]))
+    s = lfts.System(p["N"], p["NA"], 17.0, p["C"], p["dt"], p["m"], p["L"])
+    s.set_fields(fields)
+    lnQ = s.calc_concs()
+    phi = s.get_fields()[2 * M:]
+    assert abs(lnQ - float(g["lnQ"])) < FP64_TOL * abs(float(g["lnQ"]))
+    assert rel_err(phi[g["phi_idx"]], g["phi_at"]) < FP64_TOL
+    s32 = lfts.System(p["N"], p["NA"], 17.0, p["C"], p["dt"], p["m"], p["L"], precision=lfts.LFTS_FP32_MIXED)
+    s32.set_fields(fields)
+    s32.calc_concs()
+    assert rel_err(s32.get_fields()[2 * M:][g["phi_idx"]], g["phi_at"]) < FP32_PHI_TOL
+
+
+@pytest.mark.parametrize("m,N,NA", [((32, 32, 32), 12, 5), ((48, 48, 48), 6, 3), ((64, 64, 64), 5, 2),
+                                    ((96, 96, 96), 4, 2), ((128, 128, 128), 3, 1)])
+def test_calc_concs_fp64_matches_oracle_live(lfts, oracle_built, m, N, NA):
+    from pyoracle import Oracle
+    M = int(np.prod(m))
+    L = (m[0] / 16.0, m[1] / 16.0 * 1.05, m[2] / 16.0 * 0.95)
+    rng = np.random.default_rng(M)
+    w = np.zeros(4 * M)
+    w[: 2 * M] = rng.normal(0, 1.0, 2 * M)
+    o = Oracle(NA, N - NA, m, L, threads=8)
+    lnQ_ref = o.calc_concs(w)
+    s = lfts.System(N, NA, 14.0, 50.0, 0.5, m, L)
+    s.set_fields(w[: 2 * M])
+    lnQ = s.calc_concs()
+    assert abs(lnQ - lnQ_ref) < FP64_TOL * max(1.0, abs(lnQ_ref))
+    assert rel_err(s.get_fields()[2 * M:], w[2 * M:]) < FP64_TOL
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_full_size_identities_128(lfts, precision):
+    """At the headline size (128^3, N=64, NA=25): the discrete-chain identities
+    mean(phi+) = 1 and mean(phi-) = (NA-NB)/N, and FP32-mixed vs FP64 phi."""
+    m, N, NA = (128, 128, 128), 64, 25
+    M = int(np.prod(m))
+    rng = np.random.default_rng(3)
+    w2 = rng.normal(0.0, 0.5, 2 * M)
+    s = lfts.System(N, NA, 20.0, 100.0, 0.5, m, (8.0, 8.0, 8.0), precision=precision)
+    s.set_fields(w2)
+    s.calc_concs()
+    w = s.get_fields()
+    tol = 1e-11 if precision == 0 else 1e-6
+    assert abs(w[3 * M:].mean() - 1.0) < tol
+    assert abs(w[2 * M:3 * M].mean() - (2 * NA - N) / N) < tol
+    if precision == 1:
+        s64 = lfts.System(N, NA, 20.0, 100.0, 0.5, m, (8.0, 8.0, 8.0))
+        s64.set_fields(w2)
+        s64.calc_concs()
+        assert rel_err(w[2 * M:], s64.get_fields()[2 * M:]) < FP32_PHI_TOL
