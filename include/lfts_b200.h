@@ -113,6 +113,26 @@ int lfts_step_fwd(lfts_ctx *ctx, const double *q_in, double *q_out, const double
 /* step::update_g_lookup (src/step.cc:69-89): the Mk Boltzmann weights g(k) */
 int lfts_g_lookup(lfts_ctx *ctx, double *g_host);
 
+/* ---- allocation-free contour step ----------------------------------------- */
+/* Largest spectrum the allocation-free step holds: 2*mx*my*(mz/2+1) complex
+ * doubles (every mesh up to 64^3), about 4.3 MB of static device memory. */
+#define LFTS_NOALLOC_MAX_SPECTRUM (2LL * 64 * 64 * 33)
+
+/* No counterpart in the reference: the contour step of step::fwd for callers
+ * that cannot allocate device memory (their device memory comes from a pool
+ * or framework that owns all allocations, or they run where allocation is not
+ * allowed).  Needs no context and allocates nothing: q_in, q_out, h are the
+ * caller's DEVICE arrays (2M doubles each, layout of src/step.h:40-42), and the
+ * step's scratch is one static device array per GPU, holding meshes up to
+ * LFTS_NOALLOC_MAX_SPECTRUM (larger meshes return LFTS_ERR_ARG).  FP64 only.
+ * Work is enqueued on `stream` (a cudaStream_t; 0 = legacy default stream) of
+ * the current device and the call returns without waiting.  All calls on a
+ * device share that array, so calls whose kernels overlap on the GPU race:
+ * serialise them.  The first call on each device sets up the array's address;
+ * make it before any stream capture. */
+int lfts_step_fwd_noalloc(const lfts_params *p, const double *q_in, double *q_out,
+                          const double *h, int i, void *stream);
+
 /* ---- timing / integration helpers -------------------------------------- */
 /* The CUDA stream every call of this context runs on (a cudaStream_t). */
 void *lfts_stream(lfts_ctx *ctx);

@@ -93,6 +93,9 @@ inline int signed_k(int K, int m) { return (K <= m / 2) ? K : K - m; }
 
 }  // namespace
 
+// shared with lfts_noalloc.cu, which reports through lfts_last_error_string
+void lfts_internal_set_error(const char *msg) { g_last_error = msg; }
+
 struct lfts_ctx {
     lfts_params p{};
     int prec = 0, dev = 0;
