@@ -27,6 +27,15 @@
 
 namespace lfts {
 
+// Programmatic dependent launch: the chain's kernels are launched with
+// programmatic stream serialisation, so a kernel's CTAs may start while the
+// previous kernel drains.  Each kernel loads its constant tables first, then
+// waits for the previous grid's results (griddepcontrol.wait) before touching
+// the spectrum, h, q or w, and lets its dependent launch as soon as all of its
+// own CTAs are running.  Launched without the attribute, both are no-ops.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
 enum PlaneMode : int {
     PLANE_INIT_W = 0,  // h = exp(-w/N) from the fields, store h, forward transform
     PLANE_INIT_Q = 1,  // forward transform of given real rows (q_in or W-)
@@ -59,8 +68,11 @@ struct PlaneCfg {
     // Inside a row pair the packed z line is stored with one pad slot after
     // every RZ2 slots (zpos), so the contiguous-block stages hit distinct
     // shared-memory banks; the row pitch KZP leaves room for that.
+    // KZP = 4 (mod 8): the row pairs a warp works on start on different
+    // bank halves (FP32) / are bank-neutral (FP64).
     static constexpr int ZSPAN = NZ + (NZ - 1) / RZ2;
-    static constexpr int KZP = KZ > (ZSPAN + 1) / 2 ? KZ : (ZSPAN + 1) / 2;
+    static constexpr int KZP0 = KZ > (ZSPAN + 1) / 2 ? KZ : (ZSPAN + 1) / 2;
+    static constexpr int KZP = (KZP0 + 3) / 8 * 8 + 4;
     // The kz = 0 and kz = NZ/2 columns are real along y in real space, so they
     // travel through the y transforms packed as one complex column (column 0:
     // x = kz 0, y = kz NZ/2); the y phases work on KC = NZ/2 columns.
@@ -83,6 +95,22 @@ struct PlaneCfg {
 template <int TASKS, int NT>
 struct Tpt {
     static constexpr int v = (TASKS + NT - 1) / NT;
+};
+
+// The z-line phases are warp-local: warp w owns row pairs
+// [first(w), first(w) + count(w)) for all of them, so only __syncwarp
+// separates those phases and warps run through them independently.
+template <typename C>
+struct WarpPairs {
+    static constexpr int NW = C::NT / 32;
+    static constexpr int MAXP = (C::PAIRS + NW - 1) / NW;
+    static __device__ __forceinline__ int first(int w) { return (w * C::PAIRS) / NW; }
+    static __device__ __forceinline__ int count(int w) { return ((w + 1) * C::PAIRS) / NW - first(w); }
+    // rounds a lane needs for TPQ tasks per pair
+    template <int TPQ>
+    struct Rounds {
+        static constexpr int v = (MAXP * TPQ + 31) / 32;
+    };
 };
 
 // ---------------------------------------------------------------- y phases --
@@ -202,20 +230,23 @@ __device__ __forceinline__ void y_unpack0(const cpx<T> *colbuf, cpx<T> *__restri
 // Row pair q occupies the 2*KZP slots starting at P + 2q*KZP ("region");
 // the packed line's slot s lives at region[zpos(s)], the rows' k at row[k].
 
-// Build Z = A + iB (Hermitian-extended) and run inverse stage A.  Permuting:
-// all reads happen before a barrier, then all writes.
+// Build Z = A + iB (Hermitian-extended) and run inverse stage A.  Permuting
+// inside each pair region: the warp reads everything before __syncwarp, then
+// writes.
 template <typename C, typename T>
 __device__ __forceinline__ void z_build_invA(cpx<T> *P, const cpx<T> *twz)
 {
+    using WP = WarpPairs<C>;
     constexpr int KZP = C::KZP, R1 = C::RZ1, R2 = C::RZ2, NZ = R1 * R2;
-    constexpr int TASKS = C::PAIRS * R2;
-    constexpr int TPT = Tpt<TASKS, C::NT>::v;
-    cpx<T> hold[TPT][R1];
+    constexpr int RND = WP::template Rounds<R2>::v;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q0 = WP::first(w), ntask = WP::count(w) * R2;
+    cpx<T> hold[RND][R1];
 #pragma unroll
-    for (int s = 0; s < TPT; s++) {
-        const int t = threadIdx.x + s * C::NT;
-        if (t < TASKS) {
-            const int q = t / R2, j2 = t % R2;
+    for (int s = 0; s < RND; s++) {
+        const int t = lane + 32 * s;
+        if (t < ntask) {
+            const int q = q0 + t / R2, j2 = t % R2;
             const cpx<T> *A = P + 2 * q * KZP, *B = A + KZP;
 #pragma unroll
             for (int a = 0; a < R1; a++) {
@@ -239,12 +270,12 @@ __device__ __forceinline__ void z_build_invA(cpx<T> *P, const cpx<T> *twz)
             for (int k1 = 0; k1 < R1; k1++) hold[s][k1] = ctw<1>(hold[s][k1], twz[(j2 * k1) % NZ]);
         }
     }
-    __syncthreads();
+    __syncwarp();
 #pragma unroll
-    for (int s = 0; s < TPT; s++) {
-        const int t = threadIdx.x + s * C::NT;
-        if (t < TASKS) {
-            const int q = t / R2, j2 = t % R2;
+    for (int s = 0; s < RND; s++) {
+        const int t = lane + 32 * s;
+        if (t < ntask) {
+            const int q = q0 + t / R2, j2 = t % R2;
             cpx<T> *Z = P + 2 * q * KZP;
 #pragma unroll
             for (int k1 = 0; k1 < R1; k1++) Z[C::zpos(j2 + R2 * k1)] = hold[s][k1];
@@ -259,9 +290,12 @@ template <typename C, int MODE, typename T>
 __device__ __forceinline__ void z_invB_h(cpx<T> *P, const cpx<T> *twz, const T *__restrict__ h,
                                          T *__restrict__ qrow, double &qsum)
 {
+    using WP = WarpPairs<C>;
     constexpr int KZP = C::KZP, R1 = C::RZ1, R2 = C::RZ2, NZ = R1 * R2;
-    for (int t = threadIdx.x; t < C::PAIRS * R1; t += C::NT) {
-        const int q = t / R1, k1 = t % R1;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q0 = WP::first(w), ntask = WP::count(w) * R1;
+    for (int t = lane; t < ntask; t += 32) {
+        const int q = q0 + t / R1, k1 = t % R1;
         cpx<T> *Z = P + 2 * q * KZP;
         const int ya = C::ymap(2 * q), yb = C::ymap(2 * q + 1);
         cpx<T> v[R2];
@@ -290,9 +324,12 @@ __device__ __forceinline__ void z_invB_h(cpx<T> *P, const cpx<T> *twz, const T *
 template <typename C, typename T>
 __device__ __forceinline__ void z_fwdA(cpx<T> *P)
 {
+    using WP = WarpPairs<C>;
     constexpr int KZP = C::KZP, R1 = C::RZ1, R2 = C::RZ2;
-    for (int t = threadIdx.x; t < C::PAIRS * R2; t += C::NT) {
-        const int q = t / R2, j2 = t % R2;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q0 = WP::first(w), ntask = WP::count(w) * R2;
+    for (int t = lane; t < ntask; t += 32) {
+        const int q = q0 + t / R2, j2 = t % R2;
         cpx<T> *Z = P + 2 * q * KZP;
         cpx<T> v[R1];
 #pragma unroll
@@ -307,9 +344,12 @@ __device__ __forceinline__ void z_fwdA(cpx<T> *P)
 template <typename C, typename T>
 __device__ __forceinline__ void z_fwdA_tw(cpx<T> *P, const cpx<T> *twz)
 {
+    using WP = WarpPairs<C>;
     constexpr int KZP = C::KZP, R1 = C::RZ1, R2 = C::RZ2, NZ = R1 * R2;
-    for (int t = threadIdx.x; t < C::PAIRS * R2; t += C::NT) {
-        const int q = t / R2, j2 = t % R2;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q0 = WP::first(w), ntask = WP::count(w) * R2;
+    for (int t = lane; t < ntask; t += 32) {
+        const int q = q0 + t / R2, j2 = t % R2;
         cpx<T> *Z = P + 2 * q * KZP;
         cpx<T> v[R1];
 #pragma unroll
@@ -324,9 +364,12 @@ __device__ __forceinline__ void z_fwdA_tw(cpx<T> *P, const cpx<T> *twz)
 template <typename C, typename T>
 __device__ __forceinline__ void z_fwdB(cpx<T> *P)
 {
+    using WP = WarpPairs<C>;
     constexpr int KZP = C::KZP, R1 = C::RZ1, R2 = C::RZ2;
-    for (int t = threadIdx.x; t < C::PAIRS * R1; t += C::NT) {
-        const int q = t / R1, k1 = t % R1;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q0 = WP::first(w), ntask = WP::count(w) * R1;
+    for (int t = lane; t < ntask; t += 32) {
+        const int q = q0 + t / R1, k1 = t % R1;
         cpx<T> *Z = P + 2 * q * KZP;
         cpx<T> v[R2];
 #pragma unroll
@@ -342,15 +385,17 @@ __device__ __forceinline__ void z_fwdB(cpx<T> *P)
 template <typename C, bool TRANSPOSED, typename T>
 __device__ __forceinline__ void z_unpack(cpx<T> *P)
 {
+    using WP = WarpPairs<C>;
     constexpr int KC = C::KC, KZP = C::KZP, R1 = C::RZ1, R2 = C::RZ2, NZ = R1 * R2;
-    constexpr int TASKS = C::PAIRS * KC;
-    constexpr int TPT = Tpt<TASKS, C::NT>::v;
+    constexpr int TPT = WP::template Rounds<KC>::v;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q0 = WP::first(w), ntask = WP::count(w) * KC;
     cpx<T> ha[TPT], hb[TPT];
 #pragma unroll
     for (int s = 0; s < TPT; s++) {
-        const int t = threadIdx.x + s * C::NT;
-        if (t < TASKS) {
-            const int q = t / KC, k = t % KC;
+        const int t = lane + 32 * s;
+        if (t < ntask) {
+            const int q = q0 + t / KC, k = t % KC;
             const int nk = (k == 0) ? NZ / 2 : NZ - k;  // k = 0 pairs DC with Nyquist
             const cpx<T> *Z = P + 2 * q * KZP;
             const int pk = TRANSPOSED ? R2 * (k % R1) + k / R1 : k;
@@ -367,12 +412,12 @@ __device__ __forceinline__ void z_unpack(cpx<T> *P)
             }
         }
     }
-    __syncthreads();
+    __syncwarp();
 #pragma unroll
     for (int s = 0; s < TPT; s++) {
-        const int t = threadIdx.x + s * C::NT;
-        if (t < TASKS) {
-            const int q = t / KC, k = t % KC;
+        const int t = lane + 32 * s;
+        if (t < ntask) {
+            const int q = q0 + t / KC, k = t % KC;
             P[2 * q * KZP + k] = ha[s];
             P[(2 * q + 1) * KZP + k] = hb[s];
         }
@@ -405,11 +450,17 @@ __global__ void __launch_bounds__(PlaneCfg<T, NY, NZ>::NT, PlaneCfg<T, NY, NZ>::
 
     load_tw<C>(twy, a.twy, NY);
     load_tw<C>(twz, a.twz, NZ);
+    pdl_launch_dependents();
+    pdl_wait();
 
     if (MODE == PLANE_INIT_W || MODE == PLANE_INIT_Q) {
-        // real rows (natural y order), packed two per complex line
-        for (int t = threadIdx.x; t < C::PAIRS * NZ; t += C::NT) {
-            const int q = t / NZ, z = t % NZ;
+        // real rows (natural y order), packed two per complex line; the whole
+        // z section is warp-local (see WarpPairs)
+        __syncthreads();  // twiddle tables
+        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int q0 = WarpPairs<C>::first(w), ntask = WarpPairs<C>::count(w) * NZ;
+        for (int t = lane; t < ntask; t += 32) {
+            const int q = q0 + t / NZ, z = t % NZ;
             const long long ia = plane_off + (2 * q) * NZ + z, ib = ia + NZ;
             T va, vb;
             if (MODE == PLANE_INIT_W) {
@@ -430,11 +481,11 @@ __global__ void __launch_bounds__(PlaneCfg<T, NY, NZ>::NT, PlaneCfg<T, NY, NZ>::
             }
             P[2 * q * KZP + C::zpos(z)] = {va, vb};
         }
-        __syncthreads();
+        __syncwarp();
         z_fwdA_tw<C>(P, twz);
-        __syncthreads();
+        __syncwarp();
         z_fwdB<C>(P);
-        __syncthreads();
+        __syncwarp();
         z_unpack<C, true>(P);
         __syncthreads();
         y_fwdA_tw<C>(P, twy);
@@ -452,7 +503,7 @@ __global__ void __launch_bounds__(PlaneCfg<T, NY, NZ>::NT, PlaneCfg<T, NY, NZ>::
     y_B<C, 1, false>(P, twy);
     __syncthreads();
     z_build_invA<C>(P, twz);
-    __syncthreads();
+    __syncwarp();
     const T *h = a.h + (long long)(c == 0 ? a.hsel0 : a.hsel1) * M + plane_off;
     T *qrow = a.qout + c * M + plane_off;
     double qsum = 0.0;
@@ -472,9 +523,9 @@ __global__ void __launch_bounds__(PlaneCfg<T, NY, NZ>::NT, PlaneCfg<T, NY, NZ>::
         }
         return;
     }
-    __syncthreads();
+    __syncwarp();
     z_fwdA<C>(P);
-    __syncthreads();
+    __syncwarp();
     z_unpack<C, false>(P);
     __syncthreads();
     y_B<C, -1, true>(P, twy);
@@ -525,6 +576,8 @@ __global__ void __launch_bounds__(PencilCfg<T, NX, CW>::NT) pencil_kernel(Pencil
         twx[t] = a.twx[t];
         if (MODE == PENCIL_CONV) gxs[t] = a.gx[t];  // POWER mode has no g table
     }
+    pdl_launch_dependents();
+    pdl_wait();
     __syncthreads();
 
     // X1: forward stage A from global (strided rows), twiddles, to smem

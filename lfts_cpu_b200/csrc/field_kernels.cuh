@@ -51,50 +51,98 @@ __global__ void q_finalize_kernel(const double *qpart, int n, long long M, doubl
     }
 }
 
+template <typename T, int V>
+struct VecOf;
+template <> struct VecOf<float, 4> { using type = float4; };
+template <> struct VecOf<double, 2> { using type = double2; };
+
+template <typename T, int V>
+__device__ __forceinline__ void vload(const T *p, T (&out)[V])
+{
+    using VT = typename VecOf<T, V>::type;
+    const VT v = *reinterpret_cast<const VT *>(p);
+    const T *e = reinterpret_cast<const T *>(&v);
+#pragma unroll
+    for (int j = 0; j < V; j++) out[j] = e[j];
+}
+
 // phi-/phi+ (src/diblock.cc:50-57, 85-95) and, when Dh0 != nullptr, the
 // Anderson residual Dh0 = phi+ - 1 with partial sums of Dh0*Dh0 and
-// Dh0*Dh_m, m = 1..nh (src/anderson.cc:35-55).
+// Dh0*Dh_m, m = 1..nh (src/anderson.cc:35-55).  Each thread handles V
+// consecutive mesh points with vector loads; h comes from slot 1 (= [hA|hB]).
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) concentrations_kernel(
+__global__ void __launch_bounds__(kRedThreads, 4) concentrations_kernel(
     const T *__restrict__ q, long long M, int N, int NA, const double *__restrict__ w,
     double *__restrict__ phim, double *__restrict__ phip, const double *__restrict__ Qd,
     double *__restrict__ Dh0, int nh, HistPtrs hist, double *__restrict__ partials)
 {
+    constexpr int V = sizeof(T) == 4 ? 4 : 2;
     __shared__ double sh[kRedThreads / 32];
     const double Q = Qd[0];
     const double NQ = __dmul_rn((double)N, Q);
     double acc[kRedWidth];
 #pragma unroll
     for (int m = 0; m < kRedWidth; m++) acc[m] = 0.0;
+    const long long nvec = M / V;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < M; r += stride) {
+    for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < nvec; g += stride) {
+        const long long r0 = g * V;
         // slot i holds [q_i | q^_{N+1-i}] (src/diblock.cc:19-24); slot i at q + (i-1)*2M
-        double sA = 0.0, sB = 0.0;
-        for (int i = 1; i <= N; i++) {
-            const double a = (double)q[(long long)(i - 1) * 2 * M + r];
-            const double b = (double)q[(long long)(N - i) * 2 * M + M + r];
-            if (i <= NA)
-                sA = __dadd_rn(sA, __dmul_rn(a, b));
-            else
-                sB = __dadd_rn(sB, __dmul_rn(a, b));
-        }
-        const double wm = w[r], wp = w[M + r];
-        const double hA = exp(-(wm + wp) / (double)N);
-        const double hB = exp(-(-wm + wp) / (double)N);
-        const double fA = sA / __dmul_rn(NQ, hA);
-        const double fB = sB / __dmul_rn(NQ, hB);
-        const double pm = __dsub_rn(fA, fB), pp = __dadd_rn(fA, fB);
-        phim[r] = pm;
-        phip[r] = pp;
-        if (Dh0) {
-            const double d = __dsub_rn(pp, 1.0);
-            Dh0[r] = d;
-            acc[0] = __dadd_rn(acc[0], __dmul_rn(d, d));
+        double sA[V], sB[V];
 #pragma unroll
-            for (int m = 1; m < kRedWidth; m++)
-                if (m <= nh) acc[m] = __dadd_rn(acc[m], __dmul_rn(d, hist.p[m - 1][r]));
+        for (int j = 0; j < V; j++) sA[j] = sB[j] = 0.0;
+#pragma unroll 8
+        for (int i = 1; i <= N; i++) {
+            T a[V], b[V];
+            vload<T, V>(q + (long long)(i - 1) * 2 * M + r0, a);
+            vload<T, V>(q + (long long)(N - i) * 2 * M + M + r0, b);
+            if (i <= NA) {
+#pragma unroll
+                for (int j = 0; j < V; j++) sA[j] = __dadd_rn(sA[j], __dmul_rn((double)a[j], (double)b[j]));
+            } else {
+#pragma unroll
+                for (int j = 0; j < V; j++) sB[j] = __dadd_rn(sB[j], __dmul_rn((double)a[j], (double)b[j]));
+            }
+        }
+        T hA[V], hB[V];
+        vload<T, V>(q + r0, hA);
+        vload<T, V>(q + M + r0, hB);
+        double pm[V], pp[V];
+#pragma unroll
+        for (int j = 0; j < V; j++) {
+            const double fA = sA[j] / __dmul_rn(NQ, (double)hA[j]);
+            const double fB = sB[j] / __dmul_rn(NQ, (double)hB[j]);
+            pm[j] = __dsub_rn(fA, fB);
+            pp[j] = __dadd_rn(fA, fB);
+        }
+#pragma unroll
+        for (int j = 0; j < V; j += 2) {
+            *reinterpret_cast<double2 *>(phim + r0 + j) = make_double2(pm[j], pm[j + 1]);
+            *reinterpret_cast<double2 *>(phip + r0 + j) = make_double2(pp[j], pp[j + 1]);
+        }
+        if (Dh0) {
+            double d[V];
+#pragma unroll
+            for (int j = 0; j < V; j++) {
+                d[j] = __dsub_rn(pp[j], 1.0);
+                acc[0] = __dadd_rn(acc[0], __dmul_rn(d[j], d[j]));
+            }
+#pragma unroll
+            for (int j = 0; j < V; j += 2) *reinterpret_cast<double2 *>(Dh0 + r0 + j) = make_double2(d[j], d[j + 1]);
+#pragma unroll
+            for (int m = 1; m < kRedWidth; m++) {
+                if (m <= nh) {
+#pragma unroll
+                    for (int j = 0; j < V; j += 2) {
+                        const double2 hv = *reinterpret_cast<const double2 *>(hist.p[m - 1] + r0 + j);
+                        acc[m] = __dadd_rn(acc[m], __dmul_rn(d[j], hv.x));
+                        acc[m] = __dadd_rn(acc[m], __dmul_rn(d[j + 1], hv.y));
+                    }
+                }
+            }
         }
     }
+    (void)w;
     if (!Dh0) return;
 #pragma unroll
     for (int m = 0; m < kRedWidth; m++) {

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -147,6 +148,7 @@ struct lfts_ctx {
 
     bool fields_set = false;
     bool have_concs = false;
+    bool use_pdl = true;  // LFTS_NO_PDL=1 in the environment turns it off
     long long launches = 0;
     long long mix_calls = 0, mix_iters = 0;
 };
@@ -239,12 +241,30 @@ PencilArgs<T> pencil_args(lfts_ctx *c)
     return a;
 }
 
+// Chain kernels go out with programmatic stream serialisation (see pdl_wait in
+// fft_kernels.cuh): each may be scheduled while its predecessor drains.
+template <typename K, typename A>
+void launch_pdl(lfts_ctx *c, K kernel, dim3 grid, int nt, size_t smem, const A &args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(nt);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = c->st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = c->use_pdl ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args);
+    c->launches++;
+}
+
 template <typename T>
 void launch_plane(lfts_ctx *c, int mode, const PlaneArgs<T> &a, int nchains)
 {
     const PlaneKernels<T> &pl = plane_of<T>(c);
-    pl.fn[mode]<<<dim3(c->mx, nchains), pl.nt, pl.smem, c->st>>>(a);
-    c->launches++;
+    launch_pdl(c, pl.fn[mode], dim3(c->mx, nchains), pl.nt, pl.smem, a);
 }
 
 template <typename T>
@@ -252,8 +272,7 @@ void launch_pencil(lfts_ctx *c, int mode, const PencilArgs<T> &a, int nchains)
 {
     const PencilKernels<T> &pe = pencil_of<T>(c);
     const int ncol = c->my * c->KZ;
-    pe.fn[mode]<<<dim3((ncol + pe.cw - 1) / pe.cw, nchains), pe.nt, pe.smem, c->st>>>(a);
-    c->launches++;
+    launch_pdl(c, pe.fn[mode], dim3((ncol + pe.cw - 1) / pe.cw, nchains), pe.nt, pe.smem, a);
 }
 
 inline int hsel_chain0(const lfts_ctx *c, int i) { return i < c->NA ? 0 : 1; }  // src/step.cc:53-57
@@ -667,7 +686,10 @@ int lfts_create(const lfts_params *p, int precision, int device, lfts_ctx **out)
     if (precision != LFTS_FP64 && precision != LFTS_FP32_MIXED) return LFTS_ERR_ARG;
     for (int d = 0; d < 3; d++)
         if (p->m[d] < 1 || !(p->L[d] > 0.0)) return LFTS_ERR_ARG;
-    if (!fft_length_supported(p->m[0]) || !plane_pair_supported(p->m[1], p->m[2]) || (p->m[1] % 2)) {
+    // even my and mz (row pairs, packed Nyquist column) also make M a multiple
+    // of 4, which the vectorised concentration pass relies on
+    if (!fft_length_supported(p->m[0]) || !plane_pair_supported(p->m[1], p->m[2]) || (p->m[1] % 2) ||
+        (p->m[2] % 2)) {
         g_last_error = "mesh not supported: each dimension must be one of the compiled FFT lengths";
         return LFTS_ERR_UNSUPPORTED;
     }
@@ -694,6 +716,7 @@ int lfts_create(const lfts_params *p, int precision, int device, lfts_ctx **out)
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->sms = prop.multiProcessorCount;
     c->red_blocks = c->sms * 4;
+    if (const char *e = getenv("LFTS_NO_PDL")) c->use_pdl = !(e[0] == '1');
     int rc = LFTS_OK;
     auto fail = [&](int code) {
         ctx_free(c);
