@@ -136,9 +136,9 @@ int lfts_step_fwd_noalloc(const lfts_params *p, const double *q_in, double *q_ou
 /* ---- timing / integration helpers -------------------------------------- */
 /* The CUDA stream every call of this context runs on (a cudaStream_t). */
 void *lfts_stream(lfts_ctx *ctx);
-/* Run the contour chain of one calc_concs with CUDA events around every
- * launch: mean ms of a yz-plane step kernel, of an x-pencil kernel, and the
- * whole chain (leaves the propagators of the current fields). */
+/* Time the contour chain of one calc_concs: mean ms of a yz-plane step
+ * kernel and of an x-pencil kernel (one stream, events around every launch),
+ * and ms of the whole production chain (leaves the current fields' propagators). */
 int lfts_profile_chain(lfts_ctx *ctx, double *ms_plane, double *ms_pencil, double *ms_chain);
 /* Number of kernels this context has launched so far. */
 long long lfts_kernel_launches(const lfts_ctx *ctx);

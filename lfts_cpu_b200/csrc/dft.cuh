@@ -35,6 +35,54 @@ __device__ __forceinline__ cpx<T> cmulc(cpx<T> a, cpx<T> b)
 }
 template <typename T>
 __device__ __forceinline__ cpx<T> cscale(cpx<T> a, T s) { return {a.x * s, a.y * s}; }
+// a * s + c for a real scalar s
+template <typename T>
+__device__ __forceinline__ cpx<T> cfma(cpx<T> a, T s, cpx<T> c) { return {a.x * s + c.x, a.y * s + c.y}; }
+
+// FP32 complex add/sub/scale/fma go through Blackwell's packed f32x2 pipe:
+// one instruction per complex value instead of two (rounding is the same as
+// the scalar operations'; fma is fused as the scalar path's contraction is).
+__device__ __forceinline__ unsigned long long pk2(cpx<float> a)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1,%2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+    return r;
+}
+__device__ __forceinline__ cpx<float> upk2(unsigned long long r)
+{
+    cpx<float> a;
+    asm("mov.b64 {%0,%1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+    return a;
+}
+template <>
+__device__ __forceinline__ cpx<float> cadd<float>(cpx<float> a, cpx<float> b)
+{
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
+    return upk2(r);
+}
+template <>
+__device__ __forceinline__ cpx<float> csub<float>(cpx<float> a, cpx<float> b)
+{
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
+    return upk2(r);
+}
+template <>
+__device__ __forceinline__ cpx<float> cscale<float>(cpx<float> a, float s)
+{
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2({s, s})));
+    return upk2(r);
+}
+template <>
+__device__ __forceinline__ cpx<float> cfma<float>(cpx<float> a, float s, cpx<float> c)
+{
+    unsigned long long r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(pk2(a)), "l"(pk2({s, s})), "l"(pk2(c)));
+    return upk2(r);
+}
+
 // a * (S i)
 template <int S, typename T>
 __device__ __forceinline__ cpx<T> cmul_i(cpx<T> a)
@@ -143,7 +191,7 @@ struct Dft<3, S, T> {
     {
         const T h = (T)0.86602540378443864676;  // sin(2 pi / 3)
         cpx<T> s = cadd(v[1], v[2]), d = csub(v[1], v[2]);
-        cpx<T> m = {v[0].x - (T)0.5 * s.x, v[0].y - (T)0.5 * s.y};
+        cpx<T> m = cfma(s, (T)-0.5, v[0]);
         cpx<T> r = cmul_i<S>(cscale(d, h));
         v[0] = cadd(v[0], s);
         v[1] = cadd(m, r);
@@ -175,10 +223,10 @@ struct Dft<5, S, T> {
         cpx<T> b1 = cadd(v[1], v[4]), b2 = cadd(v[2], v[3]);
         cpx<T> d1 = csub(v[1], v[4]), d2 = csub(v[2], v[3]);
         cpx<T> x0 = v[0];
-        cpx<T> p1 = {x0.x + c1 * b1.x + c2 * b2.x, x0.y + c1 * b1.y + c2 * b2.y};
-        cpx<T> p2 = {x0.x + c2 * b1.x + c1 * b2.x, x0.y + c2 * b1.y + c1 * b2.y};
-        cpx<T> q1 = cmul_i<S>(cpx<T>{s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y});
-        cpx<T> q2 = cmul_i<S>(cpx<T>{s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y});
+        cpx<T> p1 = cfma(b2, c2, cfma(b1, c1, x0));
+        cpx<T> p2 = cfma(b2, c1, cfma(b1, c2, x0));
+        cpx<T> q1 = cmul_i<S>(cfma(d2, s2, cscale(d1, s1)));
+        cpx<T> q2 = cmul_i<S>(cfma(d2, -s1, cscale(d1, s2)));
         v[0] = cadd(x0, cadd(b1, b2));
         v[1] = cadd(p1, q1);
         v[4] = csub(p1, q1);

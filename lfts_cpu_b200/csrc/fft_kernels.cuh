@@ -55,6 +55,7 @@ struct PlaneArgs {
     const cpx<T> *twy, *twz;  // exp(-2 pi i t/n) tables
     double *qpart;        // LAST: per-plane sums of chain 0
     int hsel0, hsel1;     // h half used by chain 0 / chain 1 (0 = hA, 1 = hB)
+    int cbase;            // chain index of blockIdx.y == 0 (one-chain launches)
     int nchains;
     double Nd;            // N as a double (h = exp(-w/N))
 };
@@ -442,7 +443,7 @@ __global__ void __launch_bounds__(PlaneCfg<T, NY, NZ>::NT, PlaneCfg<T, NY, NZ>::
     cpx<T> *twz = twy + NY;
     cpx<T> *colbuf = twz + NZ;
 
-    const int x = blockIdx.x, c = blockIdx.y;
+    const int x = blockIdx.x, c = blockIdx.y + a.cbase;
     const int mx = gridDim.x;
     const long long M = (long long)mx * NY * NZ;
     const long long plane_off = (long long)x * NY * NZ;
@@ -549,6 +550,7 @@ struct PencilArgs {
     double *S;                // POWER: accumulator (mx*ncol)
     int ncol;                 // my*KZ
     int KZ;
+    int cbase;                // chain index of blockIdx.y == 0
 };
 
 template <typename T, int NX, int CW>
@@ -569,7 +571,7 @@ __global__ void __launch_bounds__(PencilCfg<T, NX, CW>::NT) pencil_kernel(Pencil
     cpx<T> *twx = Tl + NX * CW;
     T *gxs = reinterpret_cast<T *>(twx + NX);
 
-    const int col0 = blockIdx.x * CW, c = blockIdx.y;
+    const int col0 = blockIdx.x * CW, c = blockIdx.y + a.cbase;
     const int ncol = a.ncol;
     cpx<T> *Sg = a.spec + (long long)c * NX * ncol;
     for (int t = threadIdx.x; t < NX; t += C::NT) {

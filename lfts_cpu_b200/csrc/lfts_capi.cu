@@ -105,6 +105,8 @@ struct lfts_ctx {
     long long M = 0, Mk = 0;
     size_t tsize = 8;  // bytes of the propagator type
     cudaStream_t st = nullptr;
+    cudaStream_t st1 = nullptr;         // chain 1 of the contour chain runs here
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int sms = 148;
 
     double *w = nullptr;       // 4M: W-, w+, phi-, phi+
@@ -148,7 +150,8 @@ struct lfts_ctx {
 
     bool fields_set = false;
     bool have_concs = false;
-    bool use_pdl = true;  // LFTS_NO_PDL=1 in the environment turns it off
+    bool use_pdl = true;      // LFTS_NO_PDL=1 in the environment turns it off
+    bool two_streams = true;  // LFTS_ONE_STREAM=1 runs both chains in each launch
     long long launches = 0;
     long long mix_calls = 0, mix_iters = 0;
 };
@@ -244,13 +247,13 @@ PencilArgs<T> pencil_args(lfts_ctx *c)
 // Chain kernels go out with programmatic stream serialisation (see pdl_wait in
 // fft_kernels.cuh): each may be scheduled while its predecessor drains.
 template <typename K, typename A>
-void launch_pdl(lfts_ctx *c, K kernel, dim3 grid, int nt, size_t smem, const A &args)
+void launch_pdl(lfts_ctx *c, K kernel, dim3 grid, int nt, size_t smem, const A &args, cudaStream_t st = nullptr)
 {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = dim3(nt);
     cfg.dynamicSmemBytes = smem;
-    cfg.stream = c->st;
+    cfg.stream = st ? st : c->st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = c->use_pdl ? 1 : 0;
@@ -261,40 +264,70 @@ void launch_pdl(lfts_ctx *c, K kernel, dim3 grid, int nt, size_t smem, const A &
 }
 
 template <typename T>
-void launch_plane(lfts_ctx *c, int mode, const PlaneArgs<T> &a, int nchains)
+void launch_plane(lfts_ctx *c, int mode, const PlaneArgs<T> &a, int nchains, cudaStream_t st = nullptr)
 {
     const PlaneKernels<T> &pl = plane_of<T>(c);
-    launch_pdl(c, pl.fn[mode], dim3(c->mx, nchains), pl.nt, pl.smem, a);
+    launch_pdl(c, pl.fn[mode], dim3(c->mx, nchains), pl.nt, pl.smem, a, st);
 }
 
 template <typename T>
-void launch_pencil(lfts_ctx *c, int mode, const PencilArgs<T> &a, int nchains)
+void launch_pencil(lfts_ctx *c, int mode, const PencilArgs<T> &a, int nchains, cudaStream_t st = nullptr)
 {
     const PencilKernels<T> &pe = pencil_of<T>(c);
     const int ncol = c->my * c->KZ;
-    launch_pdl(c, pe.fn[mode], dim3((ncol + pe.cw - 1) / pe.cw, nchains), pe.nt, pe.smem, a);
+    launch_pdl(c, pe.fn[mode], dim3((ncol + pe.cw - 1) / pe.cw, nchains), pe.nt, pe.smem, a, st);
 }
 
 inline int hsel_chain0(const lfts_ctx *c, int i) { return i < c->NA ? 0 : 1; }  // src/step.cc:53-57
 inline int hsel_chain1(const lfts_ctx *c, int i) { return i < c->NB ? 1 : 0; }  // src/step.cc:60-64
 
-// propagators of both chains for all N monomers, then Q (src/diblock.cc:36-48)
+// propagators of both chains for all N monomers, then Q (src/diblock.cc:36-48).
+// The two chains (q and q^) are independent until the concentrations, so
+// each runs its own launch sequence on its own stream (st: q, st1: q^) and
+// one chain's kernels fill the other's tails; with one stream both chains
+// share every launch.
 template <typename T>
 void enqueue_chain(lfts_ctx *c)
 {
     T *q = static_cast<T *>(c->q);
     const long long M = c->M;
     PlaneArgs<T> a = plane_args<T>(c);
-    a.qout = q;  // slot 1 = [hA | hB]
-    launch_plane<T>(c, PLANE_INIT_W, a, 2);
     PencilArgs<T> pa = pencil_args<T>(c);
-    a.h = q;
-    for (int i = 1; i < c->N; i++) {
-        launch_pencil<T>(c, PENCIL_CONV, pa, 2);
-        a.qout = q + (long long)i * 2 * M;  // slot i+1
-        a.hsel0 = hsel_chain0(c, i);
-        a.hsel1 = hsel_chain1(c, i);
-        launch_plane<T>(c, i + 1 < c->N ? PLANE_STEP : PLANE_LAST, a, 2);
+    if (!c->two_streams) {
+        a.qout = q;  // slot 1 = [hA | hB]
+        launch_plane<T>(c, PLANE_INIT_W, a, 2);
+        a.h = q;
+        for (int i = 1; i < c->N; i++) {
+            launch_pencil<T>(c, PENCIL_CONV, pa, 2);
+            a.qout = q + (long long)i * 2 * M;  // slot i+1
+            a.hsel0 = hsel_chain0(c, i);
+            a.hsel1 = hsel_chain1(c, i);
+            launch_plane<T>(c, i + 1 < c->N ? PLANE_STEP : PLANE_LAST, a, 2);
+        }
+    } else {
+        cudaEventRecord(c->ev_fork, c->st);
+        cudaStreamWaitEvent(c->st1, c->ev_fork, 0);
+        cudaStream_t sc[2] = {c->st, c->st1};
+        PlaneArgs<T> ac[2] = {a, a};
+        PencilArgs<T> pc[2] = {pa, pa};
+        for (int k = 0; k < 2; k++) {
+            ac[k].cbase = k;
+            pc[k].cbase = k;
+            ac[k].qout = q;
+            launch_plane<T>(c, PLANE_INIT_W, ac[k], 1, sc[k]);
+            ac[k].h = q;
+        }
+        for (int i = 1; i < c->N; i++) {
+            for (int k = 0; k < 2; k++) launch_pencil<T>(c, PENCIL_CONV, pc[k], 1, sc[k]);
+            for (int k = 0; k < 2; k++) {
+                ac[k].qout = q + (long long)i * 2 * M;
+                ac[k].hsel0 = hsel_chain0(c, i);
+                ac[k].hsel1 = hsel_chain1(c, i);
+                launch_plane<T>(c, i + 1 < c->N ? PLANE_STEP : PLANE_LAST, ac[k], 1, sc[k]);
+            }
+        }
+        cudaEventRecord(c->ev_join, c->st1);
+        cudaStreamWaitEvent(c->st, c->ev_join, 0);
     }
     q_finalize_kernel<<<1, 256, 0, c->st>>>(c->qpart, c->mx, M, c->Qd);
     c->launches++;
@@ -322,9 +355,9 @@ void enqueue_concs_any(lfts_ctx *c, double *Dh0, int nh, const HistPtrs &hist)
         enqueue_concs<float>(c, Dh0, nh, hist);
 }
 
-// One chain with CUDA events around every contour-step kernel; returns the
-// mean duration of the yz-plane (STEP) and x-pencil (CONV) launches and the
-// whole chain (first launch to Q).
+// One chain on one stream with CUDA events around every contour-step kernel
+// (mean duration of a yz-plane STEP and an x-pencil CONV launch, both chains
+// per launch), then the production chain timed as a whole (first launch to Q).
 template <typename T>
 int profile_chain(lfts_ctx *c, double *ms_plane, double *ms_pencil, double *ms_chain)
 {
@@ -367,8 +400,13 @@ int profile_chain(lfts_ctx *c, double *ms_plane, double *ms_pencil, double *ms_c
             npl++;
         }
     }
+    // the production chain (both streams, PDL), timed as a whole
+    CK(cudaEventRecord(ev[0], c->st));
+    enqueue_chain<T>(c);
+    CK(cudaEventRecord(ev[1], c->st));
+    CK(cudaEventSynchronize(ev[1]));
     float tc = 0.f;
-    CK(cudaEventElapsedTime(&tc, ev[4 * n], ev[4 * n + 1]));
+    CK(cudaEventElapsedTime(&tc, ev[0], ev[1]));
     for (auto &e : ev) cudaEventDestroy(e);
     *ms_pencil = pe / n;
     *ms_plane = npl ? pl / npl : 0.0;
@@ -592,6 +630,10 @@ void ctx_free(lfts_ctx *c)
     cudaFree(c->sk_bins);
     cudaFree(c->sk_out);
     cudaFree(c->sf_buf);
+    if (c->st1) cudaStreamSynchronize(c->st1);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->st1) cudaStreamDestroy(c->st1);
     if (c->st) cudaStreamDestroy(c->st);
 }
 
@@ -717,13 +759,18 @@ int lfts_create(const lfts_params *p, int precision, int device, lfts_ctx **out)
     if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->sms = prop.multiProcessorCount;
     c->red_blocks = c->sms * 4;
     if (const char *e = getenv("LFTS_NO_PDL")) c->use_pdl = !(e[0] == '1');
+    if (const char *e = getenv("LFTS_ONE_STREAM")) c->two_streams = !(e[0] == '1');
     int rc = LFTS_OK;
     auto fail = [&](int code) {
         ctx_free(c);
         delete c;
         return code;
     };
-    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) return fail(LFTS_ERR_CUDA);
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->st1, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess)
+        return fail(LFTS_ERR_CUDA);
     if (!plane_kernels(c->my, c->mz, &c->pl64) || !pencil_kernels(c->mx, &c->pe64)) return fail(LFTS_ERR_UNSUPPORTED);
     if ((rc = set_smem_attrs(c->pl64, c->pe64))) return fail(rc);
     if (precision == LFTS_FP32_MIXED) {
