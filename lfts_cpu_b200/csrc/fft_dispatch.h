@@ -23,6 +23,8 @@ struct PencilKernels {
 };
 
 // false when (ny, nz) / nx has no instantiation in this build
+// packed-chain plane kernels (fft_packed.cuh), FP32
+bool plane_c_kernels(int ny, int nz, PlaneKernels<float> *out);
 bool plane_kernels(int ny, int nz, PlaneKernels<double> *out);
 bool plane_kernels(int ny, int nz, PlaneKernels<float> *out);
 bool pencil_kernels(int nx, PencilKernels<double> *out);

@@ -1,6 +1,7 @@
 // Instantiation lists of the FFT kernels, shared by fft_fp64.cu / fft_fp32.cu.
 #pragma once
 #include "fft_dispatch.h"
+#include "fft_packed.cuh"
 
 // line lengths (each needs a Plan<> in dft.cuh)
 #define LFTS_FOR_EACH_LEN(X) X(8) X(12) X(16) X(20) X(24) X(32) X(40) X(48) X(64) X(80) X(96) X(128)
@@ -19,6 +20,18 @@ static void fill_plane(PlaneKernels<T> *o)
     o->fn[PLANE_INIT_Q] = plane_kernel<T, NY, NZ, PLANE_INIT_Q>;
     o->fn[PLANE_STEP] = plane_kernel<T, NY, NZ, PLANE_STEP>;
     o->fn[PLANE_LAST] = plane_kernel<T, NY, NZ, PLANE_LAST>;
+    o->nt = C::NT;
+    o->smem = C::SMEM;
+}
+
+template <typename T, int NY, int NZ>
+static void fill_plane_c(PlaneKernels<T> *o)
+{
+    using C = PlaneCCfg<T, NY, NZ>;
+    o->fn[PLANE_INIT_W] = plane_c_kernel<T, NY, NZ, PLANE_INIT_W>;
+    o->fn[PLANE_INIT_Q] = plane_c_kernel<T, NY, NZ, PLANE_INIT_Q>;
+    o->fn[PLANE_STEP] = plane_c_kernel<T, NY, NZ, PLANE_STEP>;
+    o->fn[PLANE_LAST] = plane_c_kernel<T, NY, NZ, PLANE_LAST>;
     o->nt = C::NT;
     o->smem = C::SMEM;
 }

@@ -84,7 +84,13 @@ struct PlaneCfg {
     static constexpr int W0 = KC * RY2 > PAIRS * RZ2 ? KC * RY2 : PAIRS * RZ2;
     static constexpr int W1 = (W0 + 127) / 128 * 128;
     static constexpr int NT = W1 > 1024 ? 1024 : W1;
-    static constexpr size_t SMEM = sizeof(cpx<T>) * (size_t)(NY * KZP + 2 * NY + NZ);
+    // z twiddles as two padded 2-D tables so lanes that differ in j2 (stage
+    // A) or k1 (stage B) hit different banks: TA[j2][k1] = TB[k1][j2] = w^(j2 k1)
+    static constexpr int TAP = RZ1 + 1, TBP = RZ2 + 1;
+    static constexpr int NTA = RZ2 * TAP, NTB = RZ1 * TBP;
+    static constexpr size_t SMEM = sizeof(cpx<T>) * (size_t)(NY * KZP + 2 * NY + NTA + NTB);
+    static __device__ __forceinline__ int ta(int j2, int k1) { return j2 * TAP + k1; }
+    static __device__ __forceinline__ int tb(int k1, int u) { return k1 * TBP + u; }
     // resident CTAs per SM the register budget is sized for (FP32 planes are
     // small enough for two)
     static constexpr int MINB = (sizeof(T) == 4 && 2 * SMEM < 200 * 1024 && NT <= 512) ? 2 : 1;
@@ -115,14 +121,18 @@ struct WarpPairs {
 };
 
 // ---------------------------------------------------------------- y phases --
-// inverse, natural -> transposed, stage A reading the global half spectrum
+// inverse, natural -> transposed, stage A reading the global half spectrum.
+// KC * RY2 <= NT, so every thread has at most one task; the loads are issued
+// by y_invA_load (before the barrier that publishes the twiddle tables) and
+// consumed by y_invA_finish.
 template <typename C, typename T>
-__device__ __forceinline__ void y_invA_global(cpx<T> *P, const cpx<T> *__restrict__ Sg, const cpx<T> *twy)
+__device__ __forceinline__ void y_invA_load(const cpx<T> *__restrict__ Sg, cpx<T> (&v)[C::RY1])
 {
-    constexpr int KZ = C::KZ, KC = C::KC, KZP = C::KZP, R1 = C::RY1, R2 = C::RY2, NY = R1 * R2;
-    for (int t = threadIdx.x; t < KC * R2; t += C::NT) {
+    constexpr int KZ = C::KZ, KC = C::KC, R1 = C::RY1, R2 = C::RY2;
+    static_assert(KC * R2 <= C::NT, "one stage-A task per thread");
+    const int t = threadIdx.x;
+    if (t < KC * R2) {
         const int col = t % KC, j2 = t / KC;
-        cpx<T> v[R1];
 #pragma unroll
         for (int a = 0; a < R1; a++) {
             v[a] = Sg[(j2 + R2 * a) * KZ + col];
@@ -131,6 +141,16 @@ __device__ __forceinline__ void y_invA_global(cpx<T> *P, const cpx<T> *__restric
                 v[a] = {v[a].x - n2.y, v[a].y + n2.x};
             }
         }
+    }
+}
+
+template <typename C, typename T>
+__device__ __forceinline__ void y_invA_finish(cpx<T> *P, cpx<T> (&v)[C::RY1], const cpx<T> *twy)
+{
+    constexpr int KC = C::KC, KZP = C::KZP, R1 = C::RY1, R2 = C::RY2, NY = R1 * R2;
+    const int t = threadIdx.x;
+    if (t < KC * R2) {
+        const int col = t % KC, j2 = t / KC;
         Dft<R1, 1, T>::run(v);
 #pragma unroll
         for (int k1 = 0; k1 < R1; k1++)
@@ -235,7 +255,7 @@ __device__ __forceinline__ void y_unpack0(const cpx<T> *colbuf, cpx<T> *__restri
 // inside each pair region: the warp reads everything before __syncwarp, then
 // writes.
 template <typename C, typename T>
-__device__ __forceinline__ void z_build_invA(cpx<T> *P, const cpx<T> *twz)
+__device__ __forceinline__ void z_build_invA(cpx<T> *P, const cpx<T> *twa)
 {
     using WP = WarpPairs<C>;
     constexpr int KZP = C::KZP, R1 = C::RZ1, R2 = C::RZ2, NZ = R1 * R2;
@@ -268,7 +288,7 @@ __device__ __forceinline__ void z_build_invA(cpx<T> *P, const cpx<T> *twz)
             }
             Dft<R1, 1, T>::run(hold[s]);
 #pragma unroll
-            for (int k1 = 0; k1 < R1; k1++) hold[s][k1] = ctw<1>(hold[s][k1], twz[(j2 * k1) % NZ]);
+            for (int k1 = 0; k1 < R1; k1++) hold[s][k1] = ctw<1>(hold[s][k1], twa[C::ta(j2, k1)]);
         }
     }
     __syncwarp();
@@ -287,15 +307,36 @@ __device__ __forceinline__ void z_build_invA(cpx<T> *P, const cpx<T> *twz)
 // Inverse stage B -> real rows (transposed z order), times h, store q;
 // STEP: then forward stage B with twiddles back into smem.
 // LAST: accumulate chain-0 values into *qsum instead.
+// All of a lane's h values are loaded before its first task (they do not
+// depend on shared memory), and q goes out with evict-first stores: it is
+// read again only by the concentration pass.
 template <typename C, int MODE, typename T>
-__device__ __forceinline__ void z_invB_h(cpx<T> *P, const cpx<T> *twz, const T *__restrict__ h,
+__device__ __forceinline__ void z_invB_h(cpx<T> *P, const cpx<T> *twb, const T *__restrict__ h,
                                          T *__restrict__ qrow, double &qsum)
 {
     using WP = WarpPairs<C>;
     constexpr int KZP = C::KZP, R1 = C::RZ1, R2 = C::RZ2, NZ = R1 * R2;
+    constexpr int RND = WP::template Rounds<R1>::v;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int q0 = WP::first(w), ntask = WP::count(w) * R1;
-    for (int t = lane; t < ntask; t += 32) {
+    T hv[RND][R2][2];
+#pragma unroll
+    for (int s = 0; s < RND; s++) {
+        const int t = lane + 32 * s;
+        if (t < ntask) {
+            const int q = q0 + t / R1, k1 = t % R1;
+            const int ya = C::ymap(2 * q), yb = C::ymap(2 * q + 1);
+#pragma unroll
+            for (int k2 = 0; k2 < R2; k2++) {
+                hv[s][k2][0] = __ldg(h + ya * NZ + k1 + R1 * k2);
+                hv[s][k2][1] = __ldg(h + yb * NZ + k1 + R1 * k2);
+            }
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < RND; s++) {
+        const int t = lane + 32 * s;
+        if (t >= ntask) continue;
         const int q = q0 + t / R1, k1 = t % R1;
         cpx<T> *Z = P + 2 * q * KZP;
         const int ya = C::ymap(2 * q), yb = C::ymap(2 * q + 1);
@@ -306,17 +347,17 @@ __device__ __forceinline__ void z_invB_h(cpx<T> *P, const cpx<T> *twz, const T *
 #pragma unroll
         for (int k2 = 0; k2 < R2; k2++) {
             const int z = k1 + R1 * k2;
-            const T a = v[k2].x * h[ya * NZ + z];
-            const T b = v[k2].y * h[yb * NZ + z];
-            qrow[ya * NZ + z] = a;
-            qrow[yb * NZ + z] = b;
+            const T a = v[k2].x * hv[s][k2][0];
+            const T b = v[k2].y * hv[s][k2][1];
+            __stcs(qrow + ya * NZ + z, a);
+            __stcs(qrow + yb * NZ + z, b);
             if (MODE == PLANE_LAST) qsum += (double)a + (double)b;
             v[k2] = {a, b};
         }
         if (MODE == PLANE_STEP) {
             Dft<R2, -1, T>::run(v);
 #pragma unroll
-            for (int u = 0; u < R2; u++) Z[C::zpos(R2 * k1 + u)] = ctw<-1>(v[u], twz[(u * k1) % NZ]);
+            for (int u = 0; u < R2; u++) Z[C::zpos(R2 * k1 + u)] = ctw<-1>(v[u], twb[C::tb(k1, u)]);
         }
     }
 }
@@ -343,7 +384,7 @@ __device__ __forceinline__ void z_fwdA(cpx<T> *P)
 
 // forward stage A with twiddles, natural -> (start of) transposed, in place
 template <typename C, typename T>
-__device__ __forceinline__ void z_fwdA_tw(cpx<T> *P, const cpx<T> *twz)
+__device__ __forceinline__ void z_fwdA_tw(cpx<T> *P, const cpx<T> *twa)
 {
     using WP = WarpPairs<C>;
     constexpr int KZP = C::KZP, R1 = C::RZ1, R2 = C::RZ2, NZ = R1 * R2;
@@ -357,7 +398,7 @@ __device__ __forceinline__ void z_fwdA_tw(cpx<T> *P, const cpx<T> *twz)
         for (int a = 0; a < R1; a++) v[a] = Z[C::zpos(j2 + R2 * a)];
         Dft<R1, -1, T>::run(v);
 #pragma unroll
-        for (int k1 = 0; k1 < R1; k1++) Z[C::zpos(j2 + R2 * k1)] = ctw<-1>(v[k1], twz[(j2 * k1) % NZ]);
+        for (int k1 = 0; k1 < R1; k1++) Z[C::zpos(j2 + R2 * k1)] = ctw<-1>(v[k1], twa[C::ta(j2, k1)]);
     }
 }
 
@@ -431,6 +472,67 @@ __device__ __forceinline__ void load_tw(cpx<T> *dst, const cpx<T> *__restrict__ 
     for (int t = threadIdx.x; t < n; t += C::NT) dst[t] = src[t];
 }
 
+// Both twiddle tables through registers: the global loads go out first (before
+// the wait on the previous kernel), the shared stores later.
+template <typename C, typename T>
+struct TwStage {
+    static constexpr int NY = C::RY1 * C::RY2, NZ = C::RZ1 * C::RZ2;
+    static constexpr int TOT = NY + C::NTA + C::NTB;
+    static constexpr int PER = (TOT + C::NT - 1) / C::NT;
+    cpx<T> r[PER];
+    // global index of table entry t (twy, then TA, then TB; pads read entry 0)
+    static __device__ __forceinline__ int src(int t)
+    {
+        if (t < NY) return t;
+        t -= NY;
+        if (t < C::NTA) {
+            const int j2 = t / C::TAP, k1 = t % C::TAP;
+            return k1 < C::RZ1 ? (j2 * k1) % NZ : 0;
+        }
+        t -= C::NTA;
+        const int k1 = t / C::TBP, u = t % C::TBP;
+        return u < C::RZ2 ? (u * k1) % NZ : 0;
+    }
+    __device__ __forceinline__ void load(const cpx<T> *__restrict__ twy_g, const cpx<T> *__restrict__ twz_g)
+    {
+#pragma unroll
+        for (int s = 0; s < PER; s++) {
+            const int t = threadIdx.x + s * C::NT;
+            if (t < NY)
+                r[s] = twy_g[t];
+            else if (t < TOT)
+                r[s] = twz_g[src(t)];
+        }
+    }
+    // twy[NY] is followed by TA and TB in shared memory
+    __device__ __forceinline__ void store(cpx<T> *twy)
+    {
+#pragma unroll
+        for (int s = 0; s < PER; s++) {
+            const int t = threadIdx.x + s * C::NT;
+            if (t < TOT) twy[t] = r[s];
+        }
+    }
+};
+
+// Pull this warp's h rows (used by z_invB_h) towards L1 while the z section
+// starts: one prefetch per 128-byte line.
+template <typename C, typename T>
+__device__ __forceinline__ void prefetch_h_rows(const T *__restrict__ h)
+{
+    using WP = WarpPairs<C>;
+    constexpr int NZ = C::RZ1 * C::RZ2;
+    constexpr int LINES_PER_ROW = (NZ * (int)sizeof(T) + 127) / 128;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q0 = WP::first(w), nrows = 2 * WP::count(w);
+    for (int t = lane; t < nrows * LINES_PER_ROW; t += 32) {
+        const int row = t / LINES_PER_ROW, line = t % LINES_PER_ROW;
+        const int p = 2 * q0 + row;
+        const char *addr = reinterpret_cast<const char *>(h + C::ymap(p) * NZ) + 128 * line;
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(addr));
+    }
+}
+
 // ------------------------------------------------------------ plane kernel --
 template <typename T, int NY, int NZ, int MODE>
 __global__ void __launch_bounds__(PlaneCfg<T, NY, NZ>::NT, PlaneCfg<T, NY, NZ>::MINB) plane_kernel(PlaneArgs<T> a)
@@ -440,8 +542,9 @@ __global__ void __launch_bounds__(PlaneCfg<T, NY, NZ>::NT, PlaneCfg<T, NY, NZ>::
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<T> *P = reinterpret_cast<cpx<T> *>(smem_raw);
     cpx<T> *twy = P + NY * KZP;
-    cpx<T> *twz = twy + NY;
-    cpx<T> *colbuf = twz + NZ;
+    cpx<T> *twa = twy + NY;            // TA: stage-A z twiddles
+    cpx<T> *twb = twa + C::NTA;        // TB: stage-B z twiddles
+    cpx<T> *colbuf = twb + C::NTB;
 
     const int x = blockIdx.x, c = blockIdx.y + a.cbase;
     const int mx = gridDim.x;
@@ -449,14 +552,15 @@ __global__ void __launch_bounds__(PlaneCfg<T, NY, NZ>::NT, PlaneCfg<T, NY, NZ>::
     const long long plane_off = (long long)x * NY * NZ;
     cpx<T> *Sg = a.spec + ((long long)c * mx + x) * NY * KZ;
 
-    load_tw<C>(twy, a.twy, NY);
-    load_tw<C>(twz, a.twz, NZ);
+    TwStage<C, T> tws;
+    tws.load(a.twy, a.twz);
     pdl_launch_dependents();
     pdl_wait();
 
     if (MODE == PLANE_INIT_W || MODE == PLANE_INIT_Q) {
         // real rows (natural y order), packed two per complex line; the whole
         // z section is warp-local (see WarpPairs)
+        tws.store(twy);
         __syncthreads();  // twiddle tables
         const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
         const int q0 = WarpPairs<C>::first(w), ntask = WarpPairs<C>::count(w) * NZ;
@@ -483,7 +587,7 @@ __global__ void __launch_bounds__(PlaneCfg<T, NY, NZ>::NT, PlaneCfg<T, NY, NZ>::
             P[2 * q * KZP + C::zpos(z)] = {va, vb};
         }
         __syncwarp();
-        z_fwdA_tw<C>(P, twz);
+        z_fwdA_tw<C>(P, twa);
         __syncwarp();
         z_fwdB<C>(P);
         __syncwarp();
@@ -498,17 +602,22 @@ __global__ void __launch_bounds__(PlaneCfg<T, NY, NZ>::NT, PlaneCfg<T, NY, NZ>::
     }
 
     // inverse y (natural -> transposed rows), then packed z lines
-    __syncthreads();
-    y_invA_global<C>(P, Sg, twy);
+    {
+        cpx<T> v[C::RY1];
+        y_invA_load<C>(Sg, v);
+        tws.store(twy);
+        __syncthreads();
+        y_invA_finish<C>(P, v, twy);
+    }
     __syncthreads();
     y_B<C, 1, false>(P, twy);
     __syncthreads();
-    z_build_invA<C>(P, twz);
-    __syncwarp();
     const T *h = a.h + (long long)(c == 0 ? a.hsel0 : a.hsel1) * M + plane_off;
+    z_build_invA<C>(P, twa);
+    __syncwarp();
     T *qrow = a.qout + c * M + plane_off;
     double qsum = 0.0;
-    z_invB_h<C, MODE>(P, twz, h, qrow, qsum);
+    z_invB_h<C, MODE>(P, twb, h, qrow, qsum);
     if (MODE == PLANE_LAST) {
         if (c == 0) {
             // deterministic block reduction of the plane sum
@@ -580,18 +689,26 @@ __global__ void __launch_bounds__(PencilCfg<T, NX, CW>::NT) pencil_kernel(Pencil
     }
     pdl_launch_dependents();
     pdl_wait();
-    __syncthreads();
 
-    // X1: forward stage A from global (strided rows), twiddles, to smem
-    for (int t = threadIdx.x; t < CW * R2; t += C::NT) {
+    // X1: forward stage A from global (strided rows), twiddles, to smem.  At
+    // most one task per thread (CW * R2 <= NT); its loads go out before the
+    // barrier that publishes the tables.
+    static_assert(CW * R2 <= C::NT, "one stage-A task per thread");
+    {
+        const int t = threadIdx.x;
         const int cl = t % CW, j2 = t / CW, col = col0 + cl;
-        if (col >= ncol) continue;
+        const bool act = t < CW * R2 && col < ncol;
         cpx<T> v[R1];
+        if (act) {
 #pragma unroll
-        for (int s = 0; s < R1; s++) v[s] = Sg[(long long)(j2 + R2 * s) * ncol + col];
-        Dft<R1, -1, T>::run(v);
+            for (int s = 0; s < R1; s++) v[s] = Sg[(long long)(j2 + R2 * s) * ncol + col];
+        }
+        __syncthreads();
+        if (act) {
+            Dft<R1, -1, T>::run(v);
 #pragma unroll
-        for (int k1 = 0; k1 < R1; k1++) Tl[(j2 + R2 * k1) * CW + cl] = ctw<-1>(v[k1], twx[(j2 * k1) % NX]);
+            for (int k1 = 0; k1 < R1; k1++) Tl[(j2 + R2 * k1) * CW + cl] = ctw<-1>(v[k1], twx[(j2 * k1) % NX]);
+        }
     }
     __syncthreads();
 

@@ -150,6 +150,7 @@ struct lfts_ctx {
 
     bool fields_set = false;
     bool have_concs = false;
+    bool packed = false;      // FP32: both chains as one complex field (fft_packed.cuh)
     bool use_pdl = true;      // LFTS_NO_PDL=1 in the environment turns it off
     bool two_streams = true;  // LFTS_ONE_STREAM=1 runs both chains in each launch
     long long launches = 0;
@@ -196,12 +197,13 @@ int upload_tables(lfts_ctx *c, void **tw, void **gt)
         CK(cudaMemcpy(tw[d], t.data(), sizeof(cpx<T>) * m[d], cudaMemcpyHostToDevice));
     }
     if (!gt) return LFTS_OK;
-    // g = exp(-(2 pi)^2 (kx^2/Lx^2 + ky^2/Ly^2 + kz^2/Lz^2)/(6N)) / M, factorised
-    const int n[3] = {c->mx, c->my, c->KZ};
+    // g = exp(-(2 pi)^2 (kx^2/Lx^2 + ky^2/Ly^2 + kz^2/Lz^2)/(6N)) / M, factorised;
+    // the packed (full complex) spectrum needs kz over [0, mz), signed
+    const int n[3] = {c->mx, c->my, c->packed ? c->mz : c->KZ};
     for (int d = 0; d < 3; d++) {
         std::vector<T> g(n[d]);
         for (int K = 0; K < n[d]; K++) {
-            const int k = (d == 2) ? K : signed_k(K, m[d]);
+            const int k = (d == 2 && !c->packed) ? K : signed_k(K, m[d]);
             const double ksq = (double)k * k / (c->p.L[d] * c->p.L[d]);
             double v = std::exp(-kTwoPi * kTwoPi * ksq / (6.0 * c->N));
             if (d == 2) v /= (double)c->M;
@@ -239,8 +241,8 @@ PencilArgs<T> pencil_args(lfts_ctx *c)
     a.gx = static_cast<const T *>(c->gtab[0]);
     a.gy = static_cast<const T *>(c->gtab[1]);
     a.gz = static_cast<const T *>(c->gtab[2]);
-    a.ncol = c->my * c->KZ;
-    a.KZ = c->KZ;
+    a.ncol = c->my * (c->packed ? c->mz : c->KZ);
+    a.KZ = c->packed ? c->mz : c->KZ;
     return a;
 }
 
@@ -263,19 +265,20 @@ void launch_pdl(lfts_ctx *c, K kernel, dim3 grid, int nt, size_t smem, const A &
     c->launches++;
 }
 
+// In packed mode one launch covers both chains (gridDim.y = 1).
 template <typename T>
 void launch_plane(lfts_ctx *c, int mode, const PlaneArgs<T> &a, int nchains, cudaStream_t st = nullptr)
 {
     const PlaneKernels<T> &pl = plane_of<T>(c);
-    launch_pdl(c, pl.fn[mode], dim3(c->mx, nchains), pl.nt, pl.smem, a, st);
+    launch_pdl(c, pl.fn[mode], dim3(c->mx, c->packed ? 1 : nchains), pl.nt, pl.smem, a, st);
 }
 
 template <typename T>
 void launch_pencil(lfts_ctx *c, int mode, const PencilArgs<T> &a, int nchains, cudaStream_t st = nullptr)
 {
     const PencilKernels<T> &pe = pencil_of<T>(c);
-    const int ncol = c->my * c->KZ;
-    launch_pdl(c, pe.fn[mode], dim3((ncol + pe.cw - 1) / pe.cw, nchains), pe.nt, pe.smem, a, st);
+    launch_pdl(c, pe.fn[mode], dim3((a.ncol + pe.cw - 1) / pe.cw, c->packed ? 1 : nchains), pe.nt, pe.smem, a,
+               st);
 }
 
 inline int hsel_chain0(const lfts_ctx *c, int i) { return i < c->NA ? 0 : 1; }  // src/step.cc:53-57
@@ -293,7 +296,7 @@ void enqueue_chain(lfts_ctx *c)
     const long long M = c->M;
     PlaneArgs<T> a = plane_args<T>(c);
     PencilArgs<T> pa = pencil_args<T>(c);
-    if (!c->two_streams) {
+    if (!c->two_streams || c->packed) {
         a.qout = q;  // slot 1 = [hA | hB]
         launch_plane<T>(c, PLANE_INIT_W, a, 2);
         a.h = q;
@@ -774,7 +777,9 @@ int lfts_create(const lfts_params *p, int precision, int device, lfts_ctx **out)
     if (!plane_kernels(c->my, c->mz, &c->pl64) || !pencil_kernels(c->mx, &c->pe64)) return fail(LFTS_ERR_UNSUPPORTED);
     if ((rc = set_smem_attrs(c->pl64, c->pe64))) return fail(rc);
     if (precision == LFTS_FP32_MIXED) {
-        if (!plane_kernels(c->my, c->mz, &c->pl32) || !pencil_kernels(c->mx, &c->pe32)) return fail(LFTS_ERR_UNSUPPORTED);
+        c->packed = true;
+        if (!plane_c_kernels(c->my, c->mz, &c->pl32) || !pencil_kernels(c->mx, &c->pe32))
+            return fail(LFTS_ERR_UNSUPPORTED);
         if ((rc = set_smem_attrs(c->pl32, c->pe32))) return fail(rc);
     }
     if ((rc = ctx_alloc(c))) return fail(rc == LFTS_ERR_CUDA ? LFTS_ERR_NOMEM : rc);
