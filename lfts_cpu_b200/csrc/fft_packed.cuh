@@ -182,31 +182,46 @@ __device__ __forceinline__ void pc_z_fwdB(cpx<T> *P)
     }
 }
 
-// inverse stage B -> real space (Re: chain 1, Im: chain 2) times h, store
-// both propagators; STEP: forward stage B with twiddles; LAST: chain-1 sum.
-template <typename C, int MODE, typename T>
-__device__ __forceinline__ void pc_z_invB_h(cpx<T> *P, const cpx<T> *twb, const T *__restrict__ h1,
-                                            const T *__restrict__ h2, T *__restrict__ q1, T *__restrict__ q2,
-                                            double &qsum)
-{
-    constexpr int KP = C::KP, R1 = C::RZ1, R2 = C::RZ2, NZ = R1 * R2;
-    constexpr int RND = (C::ROWS_PER_WARP * R1 + 31) / 32;
-    int r0, nr;
-    warp_rows<C>(threadIdx.x >> 5, r0, nr);
-    const int lane = threadIdx.x & 31;
-    T hv[RND][R2][2];
+// h values of this warp's stage-B tasks (rows in transposed y order); loaded
+// before the first z phase so the DRAM latency overlaps its shared-memory work.
+template <typename C, typename T>
+struct PcH {
+    static constexpr int R1 = C::RZ1, R2 = C::RZ2, NZ = R1 * R2;
+    static constexpr int RND = (C::ROWS_PER_WARP * R1 + 31) / 32;
+    T v[RND][R2][2];
+    // rounds [s0, s1) of this lane's tasks
+    __device__ __forceinline__ void load(const T *__restrict__ h1, const T *__restrict__ h2, int s0, int s1)
+    {
+        int r0, nr;
+        warp_rows<C>(threadIdx.x >> 5, r0, nr);
+        const int lane = threadIdx.x & 31;
 #pragma unroll
-    for (int s = 0; s < RND; s++) {
-        const int t = lane + 32 * s;
-        if (t < nr * R1) {
-            const int y = C::ymap(r0 + t / R1), k1 = t % R1;
+        for (int s = 0; s < RND; s++) {
+            if (s < s0 || s >= s1) continue;
+            const int t = lane + 32 * s;
+            if (t < nr * R1) {
+                const int y = C::ymap(r0 + t / R1), k1 = t % R1;
 #pragma unroll
-            for (int k2 = 0; k2 < R2; k2++) {
-                hv[s][k2][0] = __ldg(h1 + y * NZ + k1 + R1 * k2);
-                hv[s][k2][1] = __ldg(h2 + y * NZ + k1 + R1 * k2);
+                for (int k2 = 0; k2 < R2; k2++) {
+                    v[s][k2][0] = __ldg(h1 + y * NZ + k1 + R1 * k2);
+                    v[s][k2][1] = __ldg(h2 + y * NZ + k1 + R1 * k2);
+                }
             }
         }
     }
+};
+
+// inverse stage B -> real space (Re: chain 1, Im: chain 2) times h, store
+// both propagators; STEP: forward stage B with twiddles; LAST: chain-1 sum.
+template <typename C, int MODE, typename T>
+__device__ __forceinline__ void pc_z_invB_h(cpx<T> *P, const cpx<T> *twb, const PcH<C, T> &hv,
+                                            T *__restrict__ q1, T *__restrict__ q2, double &qsum)
+{
+    constexpr int KP = C::KP, R1 = C::RZ1, R2 = C::RZ2, NZ = R1 * R2;
+    constexpr int RND = PcH<C, T>::RND;
+    int r0, nr;
+    warp_rows<C>(threadIdx.x >> 5, r0, nr);
+    const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int s = 0; s < RND; s++) {
         const int t = lane + 32 * s;
@@ -221,8 +236,8 @@ __device__ __forceinline__ void pc_z_invB_h(cpx<T> *P, const cpx<T> *twb, const 
 #pragma unroll
         for (int k2 = 0; k2 < R2; k2++) {
             const int z = k1 + R1 * k2;
-            const T a = v[k2].x * hv[s][k2][0];
-            const T b = v[k2].y * hv[s][k2][1];
+            const T a = v[k2].x * hv.v[s][k2][0];
+            const T b = v[k2].y * hv.v[s][k2][1];
             __stcs(q1 + y * NZ + z, a);
             __stcs(q2 + y * NZ + z, b);
             if (MODE == PLANE_LAST) qsum += (double)a;
@@ -349,14 +364,19 @@ __global__ void __launch_bounds__(PlaneCCfg<T, NY, NZ>::NT, 1) plane_c_kernel(Pl
     pc_y_B<C, 1, false>(P, twy);
     __syncthreads();
     // z section, warp-local (rows in transposed y order)
-    pc_z_A<C, 1, true>(P, twa);
-    __syncwarp();
+    // h of the first stage-B round goes out before the first z phase, the
+    // rest after it (register budget)
+    PcH<C, T> hv;
     const T *h1 = a.h + (long long)a.hsel0 * M + plane_off;
     const T *h2 = a.h + (long long)a.hsel1 * M + plane_off;
+    hv.load(h1, h2, 0, 1);
+    pc_z_A<C, 1, true>(P, twa);
+    hv.load(h1, h2, 1, PcH<C, T>::RND);
+    __syncwarp();
     T *q1 = a.qout + plane_off;
     T *q2 = a.qout + M + plane_off;
     double qsum = 0.0;
-    pc_z_invB_h<C, MODE>(P, twb, h1, h2, q1, q2, qsum);
+    pc_z_invB_h<C, MODE>(P, twb, hv, q1, q2, qsum);
     if (MODE == PLANE_LAST) {
         __shared__ double red[C::NT / 32];
         for (int o = 16; o > 0; o >>= 1) qsum += __shfl_xor_sync(0xffffffffu, qsum, o);

@@ -151,6 +151,10 @@ struct lfts_ctx {
     bool fields_set = false;
     bool have_concs = false;
     bool packed = false;      // FP32: both chains as one complex field (fft_packed.cuh)
+    bool use_graph = true;    // LFTS_NO_GRAPH=1: launch the chain kernel by kernel
+    cudaGraph_t chain_graph = nullptr;
+    cudaGraphExec_t chain_exec = nullptr;
+    long long chain_kernels = 0;  // kernels in one replay of chain_exec
     bool use_pdl = true;      // LFTS_NO_PDL=1 in the environment turns it off
     bool two_streams = true;  // LFTS_ONE_STREAM=1 runs both chains in each launch
     long long launches = 0;
@@ -284,13 +288,65 @@ void launch_pencil(lfts_ctx *c, int mode, const PencilArgs<T> &a, int nchains, c
 inline int hsel_chain0(const lfts_ctx *c, int i) { return i < c->NA ? 0 : 1; }  // src/step.cc:53-57
 inline int hsel_chain1(const lfts_ctx *c, int i) { return i < c->NB ? 1 : 0; }  // src/step.cc:60-64
 
+template <typename T>
+void enqueue_chain_launches(lfts_ctx *c);
+
+// The chain's launches have fixed arguments for the life of the context, so
+// they are captured once into a CUDA graph (programmatic-launch edges
+// included) and replayed: one launch per calc_concs instead of ~2N.
+template <typename T>
+void enqueue_chain(lfts_ctx *c)
+{
+    if (!c->use_graph) {
+        enqueue_chain_launches<T>(c);
+        return;
+    }
+    if (!c->chain_exec) {
+        const long long before = c->launches;
+        cudaError_t e = cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            enqueue_chain_launches<T>(c);
+            cudaGraph_t g = nullptr;
+            e = cudaStreamEndCapture(c->st, &g);
+            if (e == cudaSuccess && g) e = cudaGraphInstantiate(&c->chain_exec, g, 0);
+            if (e == cudaSuccess && c->chain_exec) {
+                c->chain_graph = g;
+                c->chain_kernels = c->launches - before;
+                // upload before the first replay and let both streams drain
+                // (the first replay after a two-stream capture misordered
+                // without this on B200 / driver 580)
+                e = cudaGraphUpload(c->chain_exec, c->st);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(c->st1);
+            } else {
+                if (g) cudaGraphDestroy(g);
+                c->chain_exec = nullptr;
+            }
+        }
+        if (e != cudaSuccess) cuda_fail(e, "chain graph capture");
+        c->launches = before;
+        cudaGetLastError();  // a failed capture falls back to direct launches below
+        if (!c->chain_exec) {
+            c->use_graph = false;
+            enqueue_chain_launches<T>(c);
+            return;
+        }
+    }
+    cudaError_t e = cudaGraphLaunch(c->chain_exec, c->st);
+    if (e != cudaSuccess) {
+        cuda_fail(e, "cudaGraphLaunch(chain)");
+        fprintf(stderr, "lfts: %s\n", g_last_error.c_str());
+    }
+    c->launches += c->chain_kernels;
+}
+
 // propagators of both chains for all N monomers, then Q (src/diblock.cc:36-48).
 // The two chains (q and q^) are independent until the concentrations, so
 // each runs its own launch sequence on its own stream (st: q, st1: q^) and
 // one chain's kernels fill the other's tails; with one stream both chains
 // share every launch.
 template <typename T>
-void enqueue_chain(lfts_ctx *c)
+void enqueue_chain_launches(lfts_ctx *c)
 {
     T *q = static_cast<T *>(c->q);
     const long long M = c->M;
@@ -633,6 +689,8 @@ void ctx_free(lfts_ctx *c)
     cudaFree(c->sk_bins);
     cudaFree(c->sk_out);
     cudaFree(c->sf_buf);
+    if (c->chain_exec) cudaGraphExecDestroy(c->chain_exec);
+    if (c->chain_graph) cudaGraphDestroy(c->chain_graph);
     if (c->st1) cudaStreamSynchronize(c->st1);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
@@ -763,6 +821,7 @@ int lfts_create(const lfts_params *p, int precision, int device, lfts_ctx **out)
     c->red_blocks = c->sms * 4;
     if (const char *e = getenv("LFTS_NO_PDL")) c->use_pdl = !(e[0] == '1');
     if (const char *e = getenv("LFTS_ONE_STREAM")) c->two_streams = !(e[0] == '1');
+    if (const char *e = getenv("LFTS_NO_GRAPH")) c->use_graph = !(e[0] == '1');
     int rc = LFTS_OK;
     auto fail = [&](int code) {
         ctx_free(c);
