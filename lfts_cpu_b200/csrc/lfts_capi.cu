@@ -1008,8 +1008,9 @@ int lfts_sk_reset(lfts_ctx *c)
 
 int lfts_sk_bin(lfts_ctx *c, double dK, double *K_out, double *S_out, int *nbins)
 {
+    // with no samples the averages come out NaN, as the reference's division
+    // by nsamples_ = 0 does
     if (!c || !K_out || !S_out || !nbins || !(dK >= 0.0)) return LFTS_ERR_ARG;
-    if (c->nsamples < 1) return LFTS_ERR_STATE;
     DeviceGuard g(c->dev);
     if (dK != c->sk_dK) {
         int rc = sk_prepare_bins(c, dK);
@@ -1021,8 +1022,8 @@ int lfts_sk_bin(lfts_ctx *c, double dK, double *K_out, double *S_out, int *nbins
     const double M = (double)c->M;
     const double coeff = CV / (c->p.XbN * c->p.XbN * M * M);
     sk_bin_kernel<<<(c->sk_nbins + 127) / 128, 128, 0, c->st>>>(c->S, c->sk_order, c->sk_wt, c->sk_bins,
-                                                               c->sk_nbins, coeff / c->nsamples, 0.5 / c->p.XbN,
-                                                               c->sk_out);
+                                                               c->sk_nbins, coeff / (double)c->nsamples,
+                                                               0.5 / c->p.XbN, c->sk_out);
     c->launches++;
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(S_out, c->sk_out, sizeof(double) * c->sk_nbins, cudaMemcpyDeviceToHost, c->st));

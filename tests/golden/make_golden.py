@@ -131,6 +131,27 @@ def case_ref_input40(name):
     print(name, "lnQ", lnQ)
 
 
+def case_program_run(name, hdr):
+    """The reference program itself (oracle/_ref/lfts-ref) on one input: its
+    stdout and every output file, packed as tests/golden/<name>.tar.gz."""
+    import subprocess
+    import tarfile
+    from pyoracle import REF_BIN
+    work = tempfile.mkdtemp()
+    try:
+        write_input(os.path.join(work, "input"), hdr)
+        out = subprocess.run([REF_BIN, "input"], cwd=work, capture_output=True, text=True,
+                             env=dict(os.environ, OMP_NUM_THREADS="4"), check=True).stdout
+        with open(os.path.join(work, "stdout.txt"), "w") as f:
+            f.write(out)
+        with tarfile.open(os.path.join(HERE, name + ".tar.gz"), "w:gz") as tar:
+            for fn in sorted(os.listdir(work)):
+                tar.add(os.path.join(work, fn), arcname=fn)
+        print(name, sorted(os.listdir(work)))
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
 def main():
     build_oracle(ref=True)
     if not RefHarness.available():
@@ -149,6 +170,12 @@ def main():
     case_trajectory("traj_lam24", ((24, 12, 16.0, 100.0, 0.5, 0), ((24, 24, 24), (3.6, 3.6, 3.6)),
                                    (2, 2, 1, 1000, 2)), 2, 2, sample_every=1)
     case_ref_input40("ref_input40")
+    # the reference CI's valgrind input, run by the reference program itself
+    case_program_run("prog_valgrind16", ((90, 40, 13.15, 100.0, 1.0, 1), ((16, 16, 16), (4.38, 4.38, 4.38)),
+                                         (1, 1, 1, 1000, 3)))
+    # a disordered-start run that saves and samples every step
+    case_program_run("prog_saves16", ((16, 6, 12.0, 50.0, 0.5, 0), ((16, 16, 16), (3.0, 3.0, 3.0)),
+                                      (2, 2, 1, 1, 0)))
 
 
 if __name__ == "__main__":
