@@ -113,6 +113,20 @@ int lfts_step_fwd(lfts_ctx *ctx, const double *q_in, double *q_out, const double
 /* step::update_g_lookup (src/step.cc:69-89): the Mk Boltzmann weights g(k) */
 int lfts_g_lookup(lfts_ctx *ctx, double *g_host);
 
+/* ---- adjoint ------------------------------------------------------------- */
+/* Gradients of the reference's H (src/lfts_simulation.cc:122-135) for the
+ * current fields: dH/dL[3] (box lengths, mesh-point fields held fixed) and
+ * dH/dXbN (bare chi N), plus H itself.  The reference has no such method (its
+ * lfts_params.h:4-6 anticipates box-altering moves that need it).  dH/dL comes
+ * from the forward and complementary propagators, the latter being the adjoint
+ * chain: dQ/dL_a = (1/M) sum_i sum_k dg/dL_a Re[q_i(k) conj(q^_{i+1}(k))].
+ * ckpt_every = 0 uses every stored propagator (and leaves phi of the fields);
+ * ckpt_every = K > 0 keeps q only at every K-th monomer and recomputes the
+ * segments in between (q^ kept in full; phi is not produced).  For an input
+ * with effective chi (isXeN = 1) the caller adds dH/dXbN * dXbN/dL through
+ * z_inf.  FP64 contexts only. */
+int lfts_backward(lfts_ctx *ctx, int ckpt_every, double *dH_dL, double *dH_dXbN, double *H);
+
 /* ---- allocation-free contour step ----------------------------------------- */
 /* Largest spectrum the allocation-free step holds: 2*mx*my*(mz/2+1) complex
  * doubles (every mesh up to 64^3), about 4.3 MB of static device memory. */

@@ -176,6 +176,14 @@ class System:
         check(lib().lfts_get_H(self._h, C.byref(v)), "lfts_get_H")
         return v.value
 
+    def backward(self, ckpt_every: int = 0):
+        """(dH/dL[3], dH/dXbN, H) for the current fields (FP64 contexts)."""
+        dL = np.empty(3)
+        dX = C.c_double()
+        H = C.c_double()
+        check(lib().lfts_backward(self._h, int(ckpt_every), dL, C.byref(dX), C.byref(H)), "lfts_backward")
+        return dL, dX.value, H.value
+
     def step_fwd(self, q_in: np.ndarray, h: np.ndarray, i: int) -> np.ndarray:
         out = np.empty(2 * self.M)
         check(lib().lfts_step_fwd(self._h, np.ascontiguousarray(q_in, np.float64), out,

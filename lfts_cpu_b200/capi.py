@@ -73,6 +73,7 @@ SIGNATURES = {
     "lfts_g_lookup": (C.c_int, [_P, _dp]),
     "lfts_step_fwd_noalloc": (C.c_int, [C.POINTER(Params), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                         C.c_void_p]),
+    "lfts_backward": (C.c_int, [_P, C.c_int, _dp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "lfts_stream": (C.c_void_p, [_P]),
     "lfts_kernel_launches": (C.c_longlong, [_P]),
     "lfts_profile_chain": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),

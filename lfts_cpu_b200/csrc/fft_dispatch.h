@@ -3,6 +3,7 @@
 #pragma once
 #include <cstddef>
 
+#include "adjoint.cuh"
 #include "fft_kernels.cuh"
 
 namespace lfts {
@@ -29,6 +30,15 @@ bool plane_kernels(int ny, int nz, PlaneKernels<double> *out);
 bool plane_kernels(int ny, int nz, PlaneKernels<float> *out);
 bool pencil_kernels(int nx, PencilKernels<double> *out);
 bool pencil_kernels(int nx, PencilKernels<float> *out);
+struct AdjKernel {
+    void (*fn)(AdjArgs);
+    int nt;
+    size_t smem;
+    int cw;
+};
+// adjoint x-pencil (FP64) for line length nx
+bool adjoint_kernel(int nx, AdjKernel *out);
+
 // line lengths with a two-stage plan
 bool fft_length_supported(int n);
 // (ny, nz) plane pairs with an instantiation

@@ -23,3 +23,21 @@ bool plane_pair_supported(int ny, int nz)
     return false;
 }
 }  // namespace lfts
+
+namespace lfts {
+bool adjoint_kernel(int nx, AdjKernel *o)
+{
+    constexpr int CW = 16;
+#define LFTS_ADJ_CASE(a)                                       \
+    if (nx == a) {                                             \
+        o->fn = pencil_adj_kernel<a, CW>;                      \
+        o->nt = AdjCfg<a, CW>::NT;                             \
+        o->smem = AdjCfg<a, CW>::SMEM;                         \
+        o->cw = CW;                                            \
+        return true;                                           \
+    }
+    LFTS_FOR_EACH_LEN(LFTS_ADJ_CASE)
+#undef LFTS_ADJ_CASE
+    return false;
+}
+}  // namespace lfts

@@ -142,6 +142,10 @@ struct lfts_ctx {
     std::vector<double> sk_K;  // K value reported for each bin
 
     void *sf_buf = nullptr;    // step_fwd scratch: q_in, q_out, h (2M each, FP64)
+    double *adj_partial = nullptr;  // adjoint block partials [blocks][3]
+    double *adj_buf = nullptr;      // checkpointed adjoint: recomputed q segment + discard row
+    int adj_buf_slots = 0;
+    AdjKernel adj{};
 
     PlaneKernels<double> pl64{};
     PencilKernels<double> pe64{};
@@ -689,6 +693,8 @@ void ctx_free(lfts_ctx *c)
     cudaFree(c->sk_bins);
     cudaFree(c->sk_out);
     cudaFree(c->sf_buf);
+    cudaFree(c->adj_partial);
+    cudaFree(c->adj_buf);
     if (c->chain_exec) cudaGraphExecDestroy(c->chain_exec);
     if (c->chain_graph) cudaGraphDestroy(c->chain_graph);
     if (c->st1) cudaStreamSynchronize(c->st1);
@@ -751,6 +757,92 @@ int step_fwd_impl(lfts_ctx *c, const double *q_in, double *q_out, const double *
     CK(cudaMemcpyAsync(q_out, dout, sizeof(double) * 2 * M, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     return LFTS_OK;
+}
+
+}  // namespace
+
+namespace {
+
+// One adjoint term: forward transforms of q_i (chain 0) and q^_{i+1}
+// (chain 1), then the k^2-weighted products summed into c->adj_partial.
+int adjoint_term(lfts_ctx *c, const double *q_i, const double *qh_ip1)
+{
+    PlaneArgs<double> a = plane_args<double>(c);
+    a.src = q_i;
+    a.src_stride = (long long)(qh_ip1 - q_i);
+    launch_plane<double>(c, PLANE_INIT_Q, a, 2);
+    AdjArgs aa{};
+    aa.spec = static_cast<const cpx<double> *>(c->spec);
+    aa.twx = static_cast<const cpx<double> *>(c->tw[0]);
+    aa.gx = static_cast<const double *>(c->gtab[0]);
+    aa.gy = static_cast<const double *>(c->gtab[1]);
+    aa.gz = static_cast<const double *>(c->gtab[2]);
+    aa.ncol = c->my * c->KZ;
+    aa.KZ = c->KZ;
+    aa.mx = c->mx;
+    aa.my = c->my;
+    aa.mz = c->mz;
+    aa.partial = c->adj_partial;
+    c->adj.fn<<<(aa.ncol + c->adj.cw - 1) / c->adj.cw, c->adj.nt, c->adj.smem, c->st>>>(aa);
+    c->launches++;
+    return LFTS_OK;
+}
+
+// Propagators of both chains with q stored only at monomers 1, 1+K, 1+2K, ...
+// (q^ in full); returns after Q is reduced.  Chains run as separate launches
+// so each output can be placed independently.
+int chain_checkpointed(lfts_ctx *c, int K)
+{
+    double *q = static_cast<double *>(c->q);
+    const long long M = c->M;
+    double *discard = c->adj_buf + (long long)K * M;
+    PlaneArgs<double> a = plane_args<double>(c);
+    PencilArgs<double> pa = pencil_args<double>(c);
+    a.qout = q;
+    launch_plane<double>(c, PLANE_INIT_W, a, 2);  // slot 1 = [hA | hB]
+    a.h = q;
+    PlaneArgs<double> a0 = a, a1 = a;
+    PencilArgs<double> p0 = pa, p1 = pa;
+    a0.cbase = 0;
+    a1.cbase = 1;
+    p0.cbase = 0;
+    p1.cbase = 1;
+    for (int i = 1; i < c->N; i++) {
+        launch_pencil<double>(c, PENCIL_CONV, p0, 1);
+        launch_pencil<double>(c, PENCIL_CONV, p1, 1);
+        const int mode = i + 1 < c->N ? PLANE_STEP : PLANE_LAST;
+        a0.hsel0 = a1.hsel0 = hsel_chain0(c, i);
+        a0.hsel1 = a1.hsel1 = hsel_chain1(c, i);
+        // q_{i+1}: a checkpoint slot or the discard row (chain 0 writes qout + 0)
+        a0.qout = (i % K == 0) ? q + (long long)i * 2 * M : discard;
+        a1.qout = q + (long long)i * 2 * M;  // q^_{N-i}: second half of slot i+1
+        launch_plane<double>(c, mode, a0, 1);
+        launch_plane<double>(c, mode, a1, 1);
+    }
+    q_finalize_kernel<<<1, 256, 0, c->st>>>(c->qpart, c->mx, M, c->Qd);
+    c->launches++;
+    return LFTS_OK;
+}
+
+// q_{c0+1} .. q_{c0+n} recomputed from the checkpoint q_{c0} into adj_buf rows 1..n
+void recompute_segment(lfts_ctx *c, const double *q_c0, int c0, int n)
+{
+    const long long M = c->M;
+    PlaneArgs<double> a = plane_args<double>(c);
+    PencilArgs<double> pa = pencil_args<double>(c);
+    a.cbase = 0;
+    pa.cbase = 0;
+    a.src = q_c0;
+    a.src_stride = 0;
+    launch_plane<double>(c, PLANE_INIT_Q, a, 1);
+    a.h = static_cast<double *>(c->q);
+    for (int j = 1; j <= n; j++) {
+        const int i = c0 + j - 1;  // step i makes q_{i+1}
+        launch_pencil<double>(c, PENCIL_CONV, pa, 1);
+        a.hsel0 = hsel_chain0(c, i);
+        a.qout = c->adj_buf + (long long)j * M;
+        launch_plane<double>(c, PLANE_STEP, a, 1);
+    }
 }
 
 }  // namespace
@@ -1082,6 +1174,73 @@ int lfts_g_lookup(lfts_ctx *c, double *g_host)
         for (int b = 0; b < c->my; b++)
             for (int k = 0; k < c->KZ; k++)
                 g_host[((long long)a * c->my + b) * c->KZ + k] = g[0][a] * g[1][b] * g[2][k];
+    return LFTS_OK;
+}
+
+int lfts_backward(lfts_ctx *c, int ckpt_every, double *dH_dL, double *dH_dXbN, double *H)
+{
+    if (!c || !dH_dL || ckpt_every < 0) return LFTS_ERR_ARG;
+    if (!c->fields_set) return LFTS_ERR_STATE;
+    if (c->prec != LFTS_FP64) {
+        g_last_error = "the adjoint runs on FP64 contexts";
+        return LFTS_ERR_UNSUPPORTED;
+    }
+    DeviceGuard g(c->dev);
+    if (!c->adj.fn && !adjoint_kernel(c->mx, &c->adj)) return LFTS_ERR_UNSUPPORTED;
+    CK(cudaFuncSetAttribute(c->adj.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->adj.smem));
+    const long long M = c->M;
+    const int nblk = (c->my * c->KZ + c->adj.cw - 1) / c->adj.cw;
+    if (!c->adj_partial) CK(cudaMalloc(&c->adj_partial, sizeof(double) * 3 * nblk));
+    CK(cudaMemsetAsync(c->adj_partial, 0, sizeof(double) * 3 * nblk, c->st));
+    double *q = static_cast<double *>(c->q);
+    const int N = c->N;
+    // q_i is the first half of slot i, q^_{i+1} the second half of slot N-i
+    auto qh = [&](int i1) { return q + (long long)(N - i1) * 2 * M + M; };  // q^_{i1}
+    if (ckpt_every == 0) {
+        int rc = calc_concs_sync(c, nullptr);
+        if (rc) return rc;
+        for (int i = 1; i < N; i++) adjoint_term(c, q + (long long)(i - 1) * 2 * M, qh(i + 1));
+    } else {
+        const int K = ckpt_every;
+        if (c->adj_buf_slots < K + 1) {
+            cudaFree(c->adj_buf);
+            c->adj_buf = nullptr;
+            CK(cudaMalloc(&c->adj_buf, sizeof(double) * (size_t)(K + 1) * M));
+            c->adj_buf_slots = K + 1;
+        }
+        chain_checkpointed(c, K);
+        for (int c0 = 1; c0 < N; c0 += K) {
+            const int last = std::min(c0 + K - 1, N - 1);  // terms i = c0 .. last
+            const double *qc = q + (long long)(c0 - 1) * 2 * M;
+            if (last > c0) recompute_segment(c, qc, c0, last - c0);
+            for (int i = c0; i <= last; i++)
+                adjoint_term(c, i == c0 ? qc : c->adj_buf + (long long)(i - c0) * M, qh(i + 1));
+        }
+        c->have_concs = false;  // phi was not recomputed
+    }
+    CK(cudaGetLastError());
+    std::vector<double> part(3 * (size_t)nblk);
+    CK(cudaMemcpyAsync(part.data(), c->adj_partial, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(c->red_host, c->Qd, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    const double Q = c->red_host[0], lnQ = c->red_host[1];
+    double S[3] = {0.0, 0.0, 0.0};
+    for (int b = 0; b < nblk; b++)
+        for (int d = 0; d < 3; d++) S[d] += part[3 * (size_t)b + d];
+    // dH/dL = -(1/Q) dQ/dL, dQ/dL_a = (1/M) 4 pi^2 S_a / (3 N L_a^3)
+    for (int d = 0; d < 3; d++) {
+        const double L = c->p.L[d];
+        dH_dL[d] = -(kTwoPi * kTwoPi * S[d] / (3.0 * N * L * L * L)) / ((double)M * Q);
+    }
+    h_sums_kernel<<<stream_grid(c), kRedThreads, 0, c->st>>>(c->w, M, c->partials);
+    reduce_partials_kernel<<<1, 256, 0, c->st>>>(c->partials, c->red_blocks, 2, c->red);
+    c->launches += 2;
+    CK(cudaMemcpyAsync(c->red_host, c->red, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    const double wp_sum = c->red_host[0], wm2_sum = c->red_host[1];
+    const double X = c->p.XbN;
+    if (dH_dXbN) *dH_dXbN = -wm2_sum / (X * X * (double)M);
+    if (H) *H = -lnQ + (wm2_sum / X - wp_sum) / (double)M;
     return LFTS_OK;
 }
 
