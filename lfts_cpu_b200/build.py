@@ -28,7 +28,6 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
            "-I" + os.path.join(ROOT, "include")] + ARCH
 CU_SOURCES = ["fft_fp64.cu", "fft_fp32.cu", "lfts_capi.cu", "lfts_noalloc.cu"]
-HEADERS = ["dft.cuh", "fft_kernels.cuh", "fft_dispatch.h", "fft_inst.cuh", "field_kernels.cuh"]
 
 
 def _nvcc() -> str:
@@ -59,7 +58,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     """Compile everything that is out of date; returns the library path."""
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
-    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "lfts_b200.h")]
+    hdrs = [os.path.join(CSRC, h) for h in sorted(os.listdir(CSRC)) if h.endswith((".cuh", ".h"))]
+    hdrs.append(os.path.join(ROOT, "include", "lfts_b200.h"))
     objs, jobs = [], []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
