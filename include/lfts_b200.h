@@ -156,6 +156,13 @@ void *lfts_stream(lfts_ctx *ctx);
 int lfts_profile_chain(lfts_ctx *ctx, double *ms_plane, double *ms_pencil, double *ms_chain);
 /* Number of kernels this context has launched so far. */
 long long lfts_kernel_launches(const lfts_ctx *ctx);
+/* Tile choices of this context's contour chain: x-pencil columns per CTA
+ * (picked at lfts_create by timing the chain for 8, 16 and 32 columns, once
+ * per precision and mesh in a process; LFTS_AUTOTUNE=0 in the environment
+ * keeps the built-in width, LFTS_PENCIL_CW=8|16|32 forces one) and yz-plane
+ * transform stages per axis (2; 3 for FP32-mixed 128 x 128 planes).  The tile
+ * width does not change results. */
+int lfts_tuning(const lfts_ctx *ctx, int *pencil_cw, int *plane_stages);
 /* Mean Anderson iteration count of all lfts_anderson_mix calls so far. */
 int lfts_anderson_stats(const lfts_ctx *ctx, long long *calls, long long *iterations);
 /* Copy the propagators of the last calc_concs, 2(N+1)M doubles (slot 0

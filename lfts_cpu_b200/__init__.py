@@ -209,6 +209,12 @@ class System:
     def kernel_launches(self) -> int:
         return int(lib().lfts_kernel_launches(self._h))
 
+    def tuning(self):
+        """(x-pencil columns per CTA, yz-plane transform stages per axis)"""
+        a, b = C.c_int(), C.c_int()
+        check(lib().lfts_tuning(self._h, C.byref(a), C.byref(b)), "lfts_tuning")
+        return a.value, b.value
+
     def profile_chain(self):
         """(ms per yz-plane step kernel, ms per x-pencil kernel, ms per chain)"""
         a, b, c = C.c_double(), C.c_double(), C.c_double()

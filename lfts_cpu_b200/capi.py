@@ -76,6 +76,7 @@ SIGNATURES = {
     "lfts_backward": (C.c_int, [_P, C.c_int, _dp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "lfts_stream": (C.c_void_p, [_P]),
     "lfts_kernel_launches": (C.c_longlong, [_P]),
+    "lfts_tuning": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "lfts_profile_chain": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "lfts_anderson_stats": (C.c_int, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "lfts_get_propagators": (C.c_int, [_P, _dp]),

@@ -4,9 +4,9 @@
 // src/step.cc:41,50): forward X[k] = sum_j x[j] exp(-2 pi i jk/n), backward
 // with +i, both unnormalised.  S = -1 selects forward, S = +1 backward.
 //
-// Radices 2, 3, 4, 5 are written out; 6, 8, 10, 12, 16 are two-level
+// Radices 2, 3, 4, 5 are written out; 6, 8, 10, 12, 16, 32 are two-level
 // Cooley-Tukey compositions of those with compile-time twiddles.  All
-// constants are exact values of cos/sin at multiples of 1.5 degrees
+// constants are exact values of cos/sin at multiples of 0.75 degrees
 // (the finest angle any supported radix needs), given to 20 digits.
 #pragma once
 #include <cuda_runtime.h>
@@ -96,23 +96,27 @@ __device__ __forceinline__ cpx<T> ctw(cpx<T> a, cpx<T> tw)
     return S < 0 ? cmul(a, tw) : cmulc(a, tw);
 }
 
-// cos and sin of 2 pi e / R for R dividing 240 (1.5-degree units).
+// cos and sin of 2 pi e / R for R dividing 480 (0.75-degree units).
 __host__ __device__ constexpr double root_cos_sin(int e, int R, bool want_sin)
 {
-    int t = ((e % R + R) % R) * (240 / R);
-    int q = t / 60, rem = t % 60;
+    int t = ((e % R + R) % R) * (480 / R);
+    int q = t / 120, rem = t % 120;
     double c = 1.0, s = 0.0;
     switch (rem) {
         case 0: c = 1.0; s = 0.0; break;
-        case 12: c = 0.95105651629515357212; s = 0.30901699437494742410; break;
-        case 15: c = 0.92387953251128675613; s = 0.38268343236508977173; break;
-        case 20: c = 0.86602540378443864676; s = 0.5; break;
-        case 24: c = 0.80901699437494742410; s = 0.58778525229247312917; break;
-        case 30: c = 0.70710678118654752440; s = 0.70710678118654752440; break;
-        case 36: c = 0.58778525229247312917; s = 0.80901699437494742410; break;
-        case 40: c = 0.5; s = 0.86602540378443864676; break;
-        case 45: c = 0.38268343236508977173; s = 0.92387953251128675613; break;
-        case 48: c = 0.30901699437494742410; s = 0.95105651629515357212; break;
+        case 15: c = 0.98078528040323044913; s = 0.19509032201612826785; break;   // 11.25
+        case 24: c = 0.95105651629515357212; s = 0.30901699437494742410; break;   // 18
+        case 30: c = 0.92387953251128675613; s = 0.38268343236508977173; break;   // 22.5
+        case 40: c = 0.86602540378443864676; s = 0.5; break;                      // 30
+        case 45: c = 0.83146961230254523708; s = 0.55557023301960222474; break;   // 33.75
+        case 48: c = 0.80901699437494742410; s = 0.58778525229247312917; break;   // 36
+        case 60: c = 0.70710678118654752440; s = 0.70710678118654752440; break;   // 45
+        case 72: c = 0.58778525229247312917; s = 0.80901699437494742410; break;   // 54
+        case 75: c = 0.55557023301960222474; s = 0.83146961230254523708; break;   // 56.25
+        case 80: c = 0.5; s = 0.86602540378443864676; break;                      // 60
+        case 90: c = 0.38268343236508977173; s = 0.92387953251128675613; break;   // 67.5
+        case 96: c = 0.30901699437494742410; s = 0.95105651629515357212; break;   // 72
+        case 105: c = 0.19509032201612826785; s = 0.98078528040323044913; break;  // 78.75
         default: c = 0.0; s = 0.0; break;  // unreachable for supported radices
     }
     double cq = q == 0 ? c : q == 1 ? -s : q == 2 ? -c : s;
@@ -141,6 +145,7 @@ template <> struct Split<8> { static constexpr int A = 4, B = 2; };
 template <> struct Split<10> { static constexpr int A = 5, B = 2; };
 template <> struct Split<12> { static constexpr int A = 4, B = 3; };
 template <> struct Split<16> { static constexpr int A = 4, B = 4; };
+template <> struct Split<32> { static constexpr int A = 8, B = 4; };
 
 template <int R, int S, typename T>
 struct Dft {

@@ -26,10 +26,16 @@ struct PencilKernels {
 // false when (ny, nz) / nx has no instantiation in this build
 // packed-chain plane kernels (fft_packed.cuh), FP32
 bool plane_c_kernels(int ny, int nz, PlaneKernels<float> *out);
+// three-stage packed-chain plane kernels (fft_plane3.cuh), FP32, 128 x 128 only
+bool plane3_kernels(int ny, int nz, PlaneKernels<float> *out);
 bool plane_kernels(int ny, int nz, PlaneKernels<double> *out);
 bool plane_kernels(int ny, int nz, PlaneKernels<float> *out);
 bool pencil_kernels(int nx, PencilKernels<double> *out);
 bool pencil_kernels(int nx, PencilKernels<float> *out);
+// x-pencil kernels of tile width cw (columns per CTA: 8, 16 or 32); the tile
+// width changes only the work split, not any column's arithmetic
+bool pencil_kernels(int nx, int cw, PencilKernels<double> *out);
+bool pencil_kernels(int nx, int cw, PencilKernels<float> *out);
 struct AdjKernel {
     void (*fn)(AdjArgs);
     int nt;

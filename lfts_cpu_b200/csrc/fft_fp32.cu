@@ -1,10 +1,18 @@
 // FP32 instantiations of the contour-step FFT kernels (the FP32-mixed path).
 #include "fft_inst.cuh"
+#include "fft_plane3.cuh"
 
 #define LFTS_PLANE_CASE_float(a, b) \
     if (ny == a && nz == b) { fill_plane<float, a, b>(o); return true; }
 #define LFTS_PENCIL_CASE_float(a) \
     if (nx == a) { fill_pencil<float, a>(o); return true; }
+#define LFTS_PENCIL_CW_CASE_float(a)                                   \
+    if (nx == a) {                                                   \
+        if (cw == 8) { fill_pencil<float, a, 8>(o); return true; }      \
+        if (cw == 16) { fill_pencil<float, a, 16>(o); return true; }    \
+        if (cw == 32) { fill_pencil<float, a, 32>(o); return true; }    \
+        return false;                                                \
+    }
 LFTS_DEFINE_DISPATCH(float)
 
 #define LFTS_PLANE_C_CASE(a, b) \
@@ -14,5 +22,16 @@ bool plane_c_kernels(int ny, int nz, PlaneKernels<float> *o)
 {
     LFTS_FOR_EACH_PAIR(LFTS_PLANE_C_CASE)
     return false;
+}
+bool plane3_kernels(int ny, int nz, PlaneKernels<float> *o)
+{
+    if (ny != 128 || nz != 128) return false;
+    o->fn[PLANE_INIT_W] = plane3_kernel<PLANE_INIT_W>;
+    o->fn[PLANE_INIT_Q] = plane3_kernel<PLANE_INIT_Q>;
+    o->fn[PLANE_STEP] = plane3_kernel<PLANE_STEP>;
+    o->fn[PLANE_LAST] = plane3_kernel<PLANE_LAST>;
+    o->nt = Plane3Cfg::NT;
+    o->smem = Plane3Cfg::SMEM;
+    return true;
 }
 }  // namespace lfts

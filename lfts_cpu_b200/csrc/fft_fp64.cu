@@ -5,6 +5,13 @@
     if (ny == a && nz == b) { fill_plane<double, a, b>(o); return true; }
 #define LFTS_PENCIL_CASE_double(a) \
     if (nx == a) { fill_pencil<double, a>(o); return true; }
+#define LFTS_PENCIL_CW_CASE_double(a)                                   \
+    if (nx == a) {                                                   \
+        if (cw == 8) { fill_pencil<double, a, 8>(o); return true; }      \
+        if (cw == 16) { fill_pencil<double, a, 16>(o); return true; }    \
+        if (cw == 32) { fill_pencil<double, a, 32>(o); return true; }    \
+        return false;                                                \
+    }
 LFTS_DEFINE_DISPATCH(double)
 
 namespace lfts {

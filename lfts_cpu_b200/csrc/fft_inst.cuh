@@ -36,10 +36,9 @@ static void fill_plane_c(PlaneKernels<T> *o)
     o->smem = C::SMEM;
 }
 
-template <typename T, int NX>
+template <typename T, int NX, int CW = 32>
 static void fill_pencil(PencilKernels<T> *o)
 {
-    constexpr int CW = 32;
     using C = PencilCfg<T, NX, CW>;
     o->fn[PENCIL_CONV] = pencil_kernel<T, NX, CW, PENCIL_CONV>;
     o->fn[PENCIL_POWER] = pencil_kernel<T, NX, CW, PENCIL_POWER>;
@@ -60,6 +59,11 @@ static void fill_pencil(PencilKernels<T> *o)
     bool pencil_kernels(int nx, PencilKernels<T> *o)                                  \
     {                                                                                 \
         LFTS_FOR_EACH_LEN(LFTS_PENCIL_CASE_##T)                                       \
+        return false;                                                                 \
+    }                                                                                 \
+    bool pencil_kernels(int nx, int cw, PencilKernels<T> *o)                          \
+    {                                                                                 \
+        LFTS_FOR_EACH_LEN(LFTS_PENCIL_CW_CASE_##T)                                    \
         return false;                                                                 \
     }                                                                                 \
     }

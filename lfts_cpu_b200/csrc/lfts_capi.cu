@@ -6,8 +6,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <numeric>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -38,6 +40,8 @@ int cuda_fail(cudaError_t e, const char *what)
     } while (0)
 
 constexpr double kTwoPi = 6.283185307179586476925286766559005768;
+// x-pencil tile widths used when autotuning is off (the usual winners at 128^3)
+constexpr int kDefaultCwFp32 = 16, kDefaultCwFp64 = 32;
 
 // Gaussian elimination with partial pivoting (first maximal |pivot|,
 // reciprocal scaling of the sub-column, right-looking rank-1 updates), then
@@ -151,6 +155,7 @@ struct lfts_ctx {
     PencilKernels<double> pe64{};
     PlaneKernels<float> pl32{};
     PencilKernels<float> pe32{};
+    int plane_stages = 2;     // yz-plane transform stages per axis (3: fft_plane3.cuh)
 
     bool fields_set = false;
     bool have_concs = false;
@@ -416,6 +421,79 @@ void enqueue_concs_any(lfts_ctx *c, double *Dh0, int nh, const HistPtrs &hist)
         enqueue_concs<double>(c, Dh0, nh, hist);
     else
         enqueue_concs<float>(c, Dh0, nh, hist);
+}
+
+// ---- x-pencil tile width ------------------------------------------------------
+// Picked by timing the whole contour chain (the pencil's cost depends on how
+// its tiles overlap the neighbouring plane kernels, so it is timed in place)
+// for each candidate width on the context's own buffers, once per precision
+// and mesh per process.  Column arithmetic does not depend on the width.
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, int> g_tuned_cw;
+
+template <typename T>
+int set_pencil(lfts_ctx *c, int cw)
+{
+    PencilKernels<T> pk{};
+    if (!pencil_kernels(c->mx, cw, &pk)) return LFTS_ERR_UNSUPPORTED;
+    for (int m = 0; m < 2; m++)
+        CK(cudaFuncSetAttribute(pk.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pk.smem));
+    pencil_of<T>(c) = pk;
+    return LFTS_OK;
+}
+
+template <typename T>
+int tune_pencil(lfts_ctx *c, int *best_cw)
+{
+    static const int cands[] = {8, 16, 32};
+    const long long launches0 = c->launches;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float best = 0.f;
+    *best_cw = 0;
+    for (int cw : cands) {
+        if (set_pencil<T>(c, cw) != LFTS_OK) continue;
+        enqueue_chain_launches<T>(c);  // warm-up
+        CK(cudaEventRecord(e0, c->st));
+        for (int r = 0; r < 3; r++) enqueue_chain_launches<T>(c);
+        CK(cudaEventRecord(e1, c->st));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (*best_cw == 0 || ms < best) {
+            best = ms;
+            *best_cw = cw;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CK(cudaStreamSynchronize(c->st));
+    c->launches = launches0;
+    return *best_cw ? LFTS_OK : LFTS_ERR_UNSUPPORTED;
+}
+
+int autotune(lfts_ctx *c)
+{
+    const bool fp64 = c->prec == LFTS_FP64;
+    int cw = fp64 ? kDefaultCwFp64 : kDefaultCwFp32;
+    const char *e = std::getenv("LFTS_AUTOTUNE");
+    const char *forced = std::getenv("LFTS_PENCIL_CW");
+    if (forced && std::atoi(forced) > 0) {
+        cw = std::atoi(forced);
+    } else if (!(e && e[0] == '0')) {
+        const auto key = std::make_tuple(c->prec, c->mx, c->my, c->mz);
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tuned_cw.find(key);
+        if (it != g_tuned_cw.end()) {
+            cw = it->second;
+        } else {
+            int rc = fp64 ? tune_pencil<double>(c, &cw) : tune_pencil<float>(c, &cw);
+            if (rc) return rc;
+            g_tuned_cw[key] = cw;
+        }
+    }
+    return fp64 ? set_pencil<double>(c, cw) : set_pencil<float>(c, cw);
 }
 
 // One chain on one stream with CUDA events around every contour-step kernel
@@ -929,8 +1007,11 @@ int lfts_create(const lfts_params *p, int precision, int device, lfts_ctx **out)
     if ((rc = set_smem_attrs(c->pl64, c->pe64))) return fail(rc);
     if (precision == LFTS_FP32_MIXED) {
         c->packed = true;
-        if (!plane_c_kernels(c->my, c->mz, &c->pl32) || !pencil_kernels(c->mx, &c->pe32))
+        if (plane3_kernels(c->my, c->mz, &c->pl32))
+            c->plane_stages = 3;
+        else if (!plane_c_kernels(c->my, c->mz, &c->pl32))
             return fail(LFTS_ERR_UNSUPPORTED);
+        if (!pencil_kernels(c->mx, kDefaultCwFp32, &c->pe32)) return fail(LFTS_ERR_UNSUPPORTED);
         if ((rc = set_smem_attrs(c->pl32, c->pe32))) return fail(rc);
     }
     if ((rc = ctx_alloc(c))) return fail(rc == LFTS_ERR_CUDA ? LFTS_ERR_NOMEM : rc);
@@ -941,6 +1022,7 @@ int lfts_create(const lfts_params *p, int precision, int device, lfts_ctx **out)
         if (!rc) rc = upload_tables<double>(c, c->sktw, nullptr);
     }
     if (rc) return fail(rc);
+    if ((rc = autotune(c))) return fail(rc);
     *out = c;
     return LFTS_OK;
 }
@@ -1254,6 +1336,14 @@ int lfts_profile_chain(lfts_ctx *c, double *ms_plane, double *ms_pencil, double 
     CK(cudaStreamSynchronize(c->st));
     if (c->prec == LFTS_FP64) return profile_chain<double>(c, ms_plane, ms_pencil, ms_chain);
     return profile_chain<float>(c, ms_plane, ms_pencil, ms_chain);
+}
+
+int lfts_tuning(const lfts_ctx *c, int *pencil_cw, int *plane_stages)
+{
+    if (!c) return LFTS_ERR_ARG;
+    if (pencil_cw) *pencil_cw = c->prec == LFTS_FP64 ? c->pe64.cw : c->pe32.cw;
+    if (plane_stages) *plane_stages = c->prec == LFTS_FP64 ? 2 : c->plane_stages;
+    return LFTS_OK;
 }
 
 long long lfts_kernel_launches(const lfts_ctx *c) { return c ? c->launches : 0; }
