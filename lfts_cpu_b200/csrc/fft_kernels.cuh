@@ -668,6 +668,12 @@ struct PencilCfg {
     static constexpr int W0 = CW * (R1 > R2 ? R1 : R2);
     static constexpr int NT = W0 >= 512 ? 256 : (W0 <= 128 ? 128 : 256);
     static constexpr size_t SMEM = sizeof(cpx<T>) * (size_t)(NX * CW + NX) + sizeof(T) * NX;
+    // FP32 tiles 8 columns wide are 64-byte rows, two to a 128-byte bank
+    // window: stage B's half-warps read rows R2 apart (same window half), so
+    // the low bit of the row index flips on alternate stage-B groups.  Stage
+    // A's row pairs {2m, 2m+1} stay together.
+    static constexpr bool SWZ = sizeof(T) == 4 && CW == 8 && R2 % 2 == 0;
+    static __device__ __forceinline__ int row(int r) { return SWZ ? (r ^ ((r / R2) & 1)) : r; }
 };
 
 template <typename T, int NX, int CW, int MODE>
@@ -707,7 +713,7 @@ __global__ void __launch_bounds__(PencilCfg<T, NX, CW>::NT) pencil_kernel(Pencil
         if (act) {
             Dft<R1, -1, T>::run(v);
 #pragma unroll
-            for (int k1 = 0; k1 < R1; k1++) Tl[(j2 + R2 * k1) * CW + cl] = ctw<-1>(v[k1], twx[(j2 * k1) % NX]);
+            for (int k1 = 0; k1 < R1; k1++) Tl[C::row(j2 + R2 * k1) * CW + cl] = ctw<-1>(v[k1], twx[(j2 * k1) % NX]);
         }
     }
     __syncthreads();
@@ -718,7 +724,7 @@ __global__ void __launch_bounds__(PencilCfg<T, NX, CW>::NT) pencil_kernel(Pencil
         if (col >= ncol) continue;
         cpx<T> v[R2];
 #pragma unroll
-        for (int u = 0; u < R2; u++) v[u] = Tl[(R2 * k1 + u) * CW + cl];
+        for (int u = 0; u < R2; u++) v[u] = Tl[C::row(R2 * k1 + u) * CW + cl];
         Dft<R2, -1, T>::run(v);
         if (MODE == PENCIL_CONV) {
             const T gyz = a.gy[col / a.KZ] * a.gz[col % a.KZ];
@@ -726,7 +732,7 @@ __global__ void __launch_bounds__(PencilCfg<T, NX, CW>::NT) pencil_kernel(Pencil
             for (int k2 = 0; k2 < R2; k2++) v[k2] = cscale(v[k2], gxs[k1 + R1 * k2] * gyz);
             Dft<R2, 1, T>::run(v);
 #pragma unroll
-            for (int u = 0; u < R2; u++) Tl[(R2 * k1 + u) * CW + cl] = ctw<1>(v[u], twx[(u * k1) % NX]);
+            for (int u = 0; u < R2; u++) Tl[C::row(R2 * k1 + u) * CW + cl] = ctw<1>(v[u], twx[(u * k1) % NX]);
         } else {
 #pragma unroll
             for (int k2 = 0; k2 < R2; k2++) {
@@ -744,7 +750,7 @@ __global__ void __launch_bounds__(PencilCfg<T, NX, CW>::NT) pencil_kernel(Pencil
         if (col >= ncol) continue;
         cpx<T> v[R1];
 #pragma unroll
-        for (int k1 = 0; k1 < R1; k1++) v[k1] = Tl[(j2 + R2 * k1) * CW + cl];
+        for (int k1 = 0; k1 < R1; k1++) v[k1] = Tl[C::row(j2 + R2 * k1) * CW + cl];
         Dft<R1, 1, T>::run(v);
 #pragma unroll
         for (int j1 = 0; j1 < R1; j1++) Sg[(long long)(j2 + R2 * j1) * ncol + col] = v[j1];

@@ -207,9 +207,10 @@ __device__ __forceinline__ void p3_s3_init(cpx<float> *P, const PlaneArgs<float>
             float v1, v2;
             if (MODE == PLANE_INIT_W) {
                 // hA = exp(-(W- + w+)/N), hB = exp(-(-W- + w+)/N)  (src/diblock.cc:64-72)
+                // (single-precision exponential: h is stored in FP32)
                 const double wm = a.w[i], wp = a.w[M + i];
-                v1 = (float)exp(-(wm + wp) / a.Nd);
-                v2 = (float)exp(-(-wm + wp) / a.Nd);
+                v1 = expf((float)(-(wm + wp) / a.Nd));
+                v2 = expf((float)(-(-wm + wp) / a.Nd));
                 a.qout[i] = v1;
                 a.qout[M + i] = v2;
             } else if (a.src) {
