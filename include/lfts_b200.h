@@ -170,6 +170,48 @@ int lfts_anderson_stats(const lfts_ctx *ctx, long long *calls, long long *iterat
 int lfts_get_propagators(lfts_ctx *ctx, double *q_host);
 
 
+/* ---- ensemble of independent replicas ------------------------------------ */
+/* Many independent FP32-mixed systems (BASELINE's batched configuration:
+ * replicas of different meshes, each with its own parameters and noise
+ * stream) advanced together.  The reference runs one system per process;
+ * there is no counterpart.  Each replica is a context of its own (buffers,
+ * tables, autotuned x-pencil width), computes exactly what a single
+ * FP32-mixed context computes when fed the same noise, and the ensemble
+ * captures one Langevin step of every replica -- update, Anderson loop with
+ * the least squares on the device, the extra calc_concs -- as one CUDA graph
+ * launch (a WHILE node runs until every replica's loop has ended).
+ * Replicas share N; meshes are 16, 24, 32, 48, 64 or 96 per side with square
+ * yz planes. */
+typedef struct lfts_ensemble lfts_ensemble;
+/* params[nrep], seeds[nrep]: the replicas' parameters and Philox streams. */
+int lfts_ensemble_create(const lfts_params *params, const unsigned long long *seeds, int nrep, int device,
+                         lfts_ensemble **out);
+int lfts_ensemble_destroy(lfts_ensemble *ens);
+/* W- and w+ of replica r (2M doubles), as lfts_set_fields. */
+int lfts_ensemble_set_fields(lfts_ensemble *ens, int r, const double *w_host);
+/* [W-, w+, phi-, phi+] of replica r (4M doubles), as lfts_get_fields. */
+int lfts_ensemble_get_fields(lfts_ensemble *ens, int r, double *w_host);
+/* Anderson mix of every replica followed by its calc_concs (the reference's
+ * start of run); k_out[nrep] (may be null) the values anderson::mix returns,
+ * lnQ_out[nrep] (may be null) ln Q of the mixed fields.  maxIter >= 2. */
+int lfts_ensemble_mix(lfts_ensemble *ens, int maxIter, double tol, int *k_out, double *lnQ_out);
+/* nsteps Langevin steps of every replica (src/lfts_simulation.cc:69-76 per
+ * replica: step_wm with on-device noise, mix, calc_concs); k_out[nsteps][nrep]
+ * (may be null; reading it synchronises after every step), lnQ_out[nrep]
+ * (may be null) after the last step.  The noise of replica r at step s is
+ * lfts_noise_philox(seeds[r], s, M, sigma_r); step 0 is the initial noise,
+ * the first call's first step is step 1. */
+int lfts_ensemble_run(lfts_ensemble *ens, int nsteps, int maxIter, double tol, int *k_out, double *lnQ_out);
+/* x-pencil columns per CTA of replica r's mesh (autotuned). */
+int lfts_ensemble_tuning(const lfts_ensemble *ens, int r, int *pencil_cw);
+/* The CUDA stream the ensemble's graphs run on (a cudaStream_t). */
+void *lfts_ensemble_stream(lfts_ensemble *ens);
+/* Kernels placed in the ensemble's graphs so far (per body iteration). */
+long long lfts_ensemble_kernel_launches(const lfts_ensemble *ens);
+/* sigma * z for points 0..n-1 of step s of Philox stream `seed`, computed on
+ * the current device (the ensemble's noise; see lfts_cpu_b200/csrc/philox.cuh). */
+int lfts_noise_philox(unsigned long long seed, long long step, long long n, double sigma, double *out_host);
+
 /* ---- host helpers with the reference driver's semantics ------------------ */
 /* Everything the reference's lfts_params derives from the 3-line input header
  * (src/lfts_params.cc:87-119). */

@@ -230,3 +230,87 @@ class System:
         v = C.c_size_t()
         check(lib().lfts_device_bytes(self._h, C.byref(v)), "lfts_device_bytes")
         return int(v.value)
+
+
+def noise_philox(seed: int, step: int, n: int, sigma: float) -> np.ndarray:
+    """sigma * N(0,1) deviates of points 0..n-1 of step `step` of Philox
+    stream `seed` (the ensemble's noise), computed on the GPU."""
+    out = np.empty(int(n))
+    check(lib().lfts_noise_philox(int(seed), int(step), int(n), float(sigma), out), "lfts_noise_philox")
+    return out
+
+
+class Ensemble:
+    """Independent FP32-mixed replicas advanced together (an lfts_ensemble).
+
+    replicas: list of dicts with keys N, NA, XbN, C, dt, m, L and seed."""
+
+    def __init__(self, replicas, device: int = 0):
+        n = len(replicas)
+        params = (Params * n)()
+        seeds = (C.c_ulonglong * n)()
+        self.M, self.m, self.sigma = [], [], []
+        for r, d in enumerate(replicas):
+            p = params[r]
+            p.N, p.NA, p.XbN, p.C, p.dt = int(d["N"]), int(d["NA"]), float(d["XbN"]), float(d["C"]), float(d["dt"])
+            for k in range(3):
+                p.m[k] = int(d["m"][k])
+                p.L[k] = float(d["L"][k])
+            seeds[r] = int(d["seed"])
+            M = int(np.prod(d["m"]))
+            self.M.append(M)
+            self.m.append(tuple(int(x) for x in d["m"]))
+            V = float(np.prod(d["L"]))
+            self.sigma.append(float(np.sqrt(2.0 * M * float(d["dt"]) / (float(d["C"]) * V))))
+        self.nrep = n
+        self.seeds = [int(d["seed"]) for d in replicas]
+        self._h = C.c_void_p()
+        check(lib().lfts_ensemble_create(C.cast(params, C.c_void_p), seeds, n, int(device), C.byref(self._h)),
+              "lfts_ensemble_create")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lfts_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_fields(self, r: int, w2: np.ndarray) -> None:
+        w2 = np.ascontiguousarray(w2[: 2 * self.M[r]], dtype=np.float64)
+        check(lib().lfts_ensemble_set_fields(self._h, int(r), w2), "lfts_ensemble_set_fields")
+
+    def get_fields(self, r: int) -> np.ndarray:
+        out = np.empty(4 * self.M[r])
+        check(lib().lfts_ensemble_get_fields(self._h, int(r), out), "lfts_ensemble_get_fields")
+        return out
+
+    def mix(self, max_iter: int = 200, tol: float = 1e-4):
+        """(K per replica, ln Q per replica)"""
+        k = np.zeros(self.nrep, dtype=np.int32)
+        lnq = np.zeros(self.nrep)
+        check(lib().lfts_ensemble_mix(self._h, int(max_iter), float(tol), k.ctypes.data, lnq.ctypes.data),
+              "lfts_ensemble_mix")
+        return k, lnq
+
+    def run(self, nsteps: int, max_iter: int = 200, tol: float = 1e-4, record_k: bool = True):
+        """(K[nsteps][nrep] or None, ln Q per replica after the last step)"""
+        k = np.zeros((nsteps, self.nrep), dtype=np.int32) if record_k else None
+        lnq = np.zeros(self.nrep)
+        check(lib().lfts_ensemble_run(self._h, int(nsteps), int(max_iter), float(tol),
+                                      k.ctypes.data if record_k else None, lnq.ctypes.data), "lfts_ensemble_run")
+        return k, lnq
+
+    def tuning(self, r: int) -> int:
+        cw = C.c_int()
+        check(lib().lfts_ensemble_tuning(self._h, int(r), C.byref(cw)), "lfts_ensemble_tuning")
+        return cw.value
+
+    def stream(self) -> int:
+        return int(lib().lfts_ensemble_stream(self._h) or 0)
+
+    def kernel_launches(self) -> int:
+        return int(lib().lfts_ensemble_kernel_launches(self._h))

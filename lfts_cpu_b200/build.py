@@ -27,7 +27,7 @@ EXE = os.path.join(PKG, "lfts-b200")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
            "-I" + os.path.join(ROOT, "include")] + ARCH
-CU_SOURCES = ["fft_fp64.cu", "fft_fp32.cu", "lfts_capi.cu", "lfts_noalloc.cu"]
+CU_SOURCES = ["fft_fp64.cu", "fft_fp32.cu", "lfts_capi.cu", "lfts_noalloc.cu", "lfts_ensemble.cu"]
 
 
 def _nvcc() -> str:

@@ -80,6 +80,16 @@ SIGNATURES = {
     "lfts_profile_chain": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "lfts_anderson_stats": (C.c_int, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "lfts_get_propagators": (C.c_int, [_P, _dp]),
+    "lfts_ensemble_create": (C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "lfts_ensemble_destroy": (C.c_int, [_P]),
+    "lfts_ensemble_set_fields": (C.c_int, [_P, C.c_int, _dp]),
+    "lfts_ensemble_get_fields": (C.c_int, [_P, C.c_int, _dp]),
+    "lfts_ensemble_mix": (C.c_int, [_P, C.c_int, C.c_double, C.c_void_p, C.c_void_p]),
+    "lfts_ensemble_run": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p]),
+    "lfts_ensemble_tuning": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
+    "lfts_ensemble_stream": (C.c_void_p, [_P]),
+    "lfts_ensemble_kernel_launches": (C.c_longlong, [_P]),
+    "lfts_noise_philox": (C.c_int, [C.c_ulonglong, C.c_longlong, C.c_longlong, C.c_double, _dp]),
     "lfts_read_input": (C.c_int, [C.c_char_p, C.POINTER(Input)]),
     "lfts_z_inf_discrete": (C.c_double, [C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_int, C.c_double,
                                          C.c_int]),

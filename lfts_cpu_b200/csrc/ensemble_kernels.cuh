@@ -1,0 +1,353 @@
+// Batched kernels of the replica ensemble (lfts_ensemble.cu): many
+// independent FP32-mixed L-FTS systems, grouped by mesh, advanced by one CUDA
+// graph launch per Langevin step.  Every replica's arithmetic is that of a
+// single FP32-mixed context (the same kernel bodies, the same reduction
+// partitions), so a replica reproduces a single context fed the same noise.
+//
+// The Anderson loop runs on the device, per replica: each body iteration of
+// the graph's WHILE node runs the contour chain, the concentrations with the
+// residual dot products, the reduction and least-squares solve, the w+
+// update and the control step.  A replica whose loop has stopped runs one
+// more chain + concentrations (the reference's extra calc_concs after mix,
+// src/lfts_simulation.cc:69-76) and then idles (its CTAs return at once)
+// until every replica is done; the control kernel ends the WHILE loop then.
+#pragma once
+#include "fft_packed.cuh"
+#include "field_kernels.cuh"
+#include "philox.cuh"
+
+namespace lfts {
+
+// device-resident descriptor of one replica (buffers owned by its context)
+struct EnsRep {
+    int mx, my, mz, N, NA, NB;
+    long long M;
+    int red_blocks;
+    double XbN, dt, sigma;
+    unsigned long long seed;
+    double *w;
+    float *q;
+    cpx<float> *spec;
+    const cpx<float> *tw[3];
+    const float *g[3];
+    double *qpart, *Qd, *partials;
+    double *Dh[kRedWidth], *wh[kRedWidth];
+    // Anderson loop state
+    int phys[kRedWidth];  // logical history slot -> physical buffer
+    int cur;              // physical buffer of the current iteration
+    int k;                // iteration number (src/anderson.cc:31)
+    int active, stopped, done, go, simple, singular;
+    int iters;            // k at loop exit (the value anderson::mix returns)
+    double coef[kMaxHist];
+    double DD[kRedWidth][kRedWidth];
+};
+
+__device__ __forceinline__ int ens_nh(int k) { return (k < kMaxHist + 1) ? k - 1 : kMaxHist; }
+
+template <int NY, int NZ, int MODE>
+__global__ void __launch_bounds__(PlaneCCfg<float, NY, NZ>::NT, 1)
+    ens_plane_kernel(EnsRep *__restrict__ reps, const int *__restrict__ members, int i)
+{
+    const EnsRep &R = reps[members[blockIdx.y]];
+    if (!R.active) return;
+    PlaneArgs<float> a{};
+    a.w = R.w;
+    a.spec = R.spec;
+    a.twy = R.tw[1];
+    a.twz = R.tw[2];
+    a.qpart = R.qpart;
+    a.nchains = 2;
+    a.Nd = (double)R.N;
+    if (MODE == PLANE_INIT_W) {
+        a.qout = R.q;  // slot 1 = [hA | hB]
+    } else {
+        a.h = R.q;
+        a.qout = R.q + (long long)i * 2 * R.M;    // slot i+1
+        a.hsel0 = i < R.NA ? 0 : 1;               // src/step.cc:53-57
+        a.hsel1 = i < R.NB ? 1 : 0;               // src/step.cc:60-64
+    }
+    plane_c_body<float, NY, NZ, MODE>(a, blockIdx.x, R.mx);
+}
+
+template <int NX, int CW>
+__global__ void __launch_bounds__(PencilCfg<float, NX, CW>::NT)
+    ens_pencil_kernel(EnsRep *__restrict__ reps, const int *__restrict__ members)
+{
+    const EnsRep &R = reps[members[blockIdx.y]];
+    if (!R.active) return;
+    PencilArgs<float> a{};
+    a.spec = R.spec;
+    a.twx = R.tw[0];
+    a.gx = R.g[0];
+    a.gy = R.g[1];
+    a.gz = R.g[2];
+    a.ncol = R.my * R.mz;
+    a.KZ = R.mz;
+    pencil_body<float, NX, CW, PENCIL_CONV>(a, blockIdx.x, 0);
+}
+
+// Q and ln Q of every active replica (as q_finalize_kernel, 256 threads)
+__global__ void __launch_bounds__(256) ens_qfinal_kernel(EnsRep *__restrict__ reps)
+{
+    const EnsRep &R = reps[blockIdx.x];
+    if (!R.active) return;
+    __shared__ double sh[32];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < R.mx; i += blockDim.x) s += R.qpart[i];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) {
+        const double Q = s / (double)R.M;
+        R.Qd[0] = Q;
+        R.Qd[1] = log(Q);
+    }
+}
+
+// phi, the residual Dh0 and its dot products: grid (max red_blocks, nrep)
+__global__ void __launch_bounds__(kRedThreads, 4) ens_conc_kernel(EnsRep *__restrict__ reps)
+{
+    const EnsRep &R = reps[blockIdx.y];
+    if (!R.active || (int)blockIdx.x >= R.red_blocks) return;
+    const int nh = ens_nh(R.k);
+    HistPtrs hist{};
+    for (int m = 1; m <= nh; m++) hist.p[m - 1] = R.Dh[R.phys[m]];
+    concentrations_body<float>(R.q, R.M, R.N, R.NA, R.w, R.w + 2 * R.M, R.w + 3 * R.M, R.Qd, R.Dh[R.cur], nh, hist,
+                               R.partials, blockIdx.x, R.red_blocks);
+}
+
+// GSL-style LU with partial pivoting and the two triangular solves
+// (src/anderson.cc:106-127) on one warp: lane i holds row i of the n x n
+// matrix (n <= kMaxHist) in registers and y[i].  Every matrix element goes
+// through the same operations in the same order as in the sequential
+// algorithm, each rounded separately (no fused multiply-adds), so x equals
+// the host's result bit for bit.  Returns false (all lanes) for an exactly
+// singular matrix.  x is valid in lane i for i < n.
+__device__ bool lu_solve_warp(double (&a)[kMaxHist], double y, double &x, int n)
+{
+    const int lane = threadIdx.x & 31;
+    int perm = lane;  // original row now at this position
+#pragma unroll
+    for (int j = 0; j < kMaxHist; j++) {
+        if (j >= n) break;
+        // first maximal |a_ij|, i >= j (scan in row order, as sequentially)
+        int piv = j;
+        double amax = fabs(__shfl_sync(0xffffffffu, a[j], j));
+        for (int i = j + 1; i < n; i++) {
+            const double v = fabs(__shfl_sync(0xffffffffu, a[j], i));
+            if (v > amax) {
+                amax = v;
+                piv = i;
+            }
+        }
+        if (piv != j) {
+            const int src = lane == j ? piv : (lane == piv ? j : lane);
+#pragma unroll
+            for (int k = 0; k < kMaxHist; k++) a[k] = __shfl_sync(0xffffffffu, a[k], src);
+            perm = __shfl_sync(0xffffffffu, perm, src);
+        }
+        if (j + 1 < n) {
+            const double ajj = __shfl_sync(0xffffffffu, a[j], j);
+            if (lane > j && lane < n) {
+                if (fabs(ajj) >= 2.2250738585072014e-308)
+                    a[j] = __dmul_rn(a[j], __ddiv_rn(1.0, ajj));
+                else
+                    a[j] = __ddiv_rn(a[j], ajj);
+            }
+#pragma unroll
+            for (int k = 0; k < kMaxHist; k++) {
+                if (k > j && k < n) {
+                    const double ajk = __shfl_sync(0xffffffffu, a[k], j);
+                    if (lane > j && lane < n) a[k] = __dsub_rn(a[k], __dmul_rn(a[j], ajk));
+                }
+            }
+        }
+    }
+    double diag = 1.0;
+#pragma unroll
+    for (int k = 0; k < kMaxHist; k++)
+        if (k == lane) diag = a[k];
+    if (__any_sync(0xffffffffu, lane < n && diag == 0.0)) return false;
+    // forward substitution (unit lower), x_j broadcast as it becomes final
+    double t = __shfl_sync(0xffffffffu, y, perm);
+#pragma unroll
+    for (int j = 0; j < kMaxHist; j++) {
+        if (j >= n) break;
+        const double xj = __shfl_sync(0xffffffffu, t, j);
+        if (lane > j && lane < n) t = __dsub_rn(t, __dmul_rn(a[j], xj));
+    }
+    // back substitution: row i subtracts a_ij x_j for j = i+1 .. n-1 in order
+    x = t;
+    for (int i = n - 1; i >= 0; i--) {
+        double ti = x;
+#pragma unroll
+        for (int j = 0; j < kMaxHist; j++) {
+            if (j > i && j < n) {
+                const double xj = __shfl_sync(0xffffffffu, x, j);
+                if (lane == i) ti = __dsub_rn(ti, __dmul_rn(a[j], xj));
+            }
+        }
+        if (lane == i) x = __ddiv_rn(ti, diag);
+    }
+    return true;
+}
+
+// One replica per block: the reduction of its dot products (as
+// reduce_partials_kernel, 256 threads, fixed order), then on one warp the
+// scalar part of the Anderson iteration (src/anderson.cc:35-89): the row
+// DD[0][0..nh], the least-squares coefficients (k >= 2), the DD bookkeeping
+// and whether the loop goes on (err > tol and k + 1 < maxIter).  In the
+// iteration after the loop stopped (the extra calc_concs) it only marks the
+// replica done.
+__global__ void __launch_bounds__(256) ens_reduce_solve_kernel(EnsRep *__restrict__ reps, double tol, int maxIter)
+{
+    EnsRep &R = reps[blockIdx.x];
+    if (!R.active) return;
+    if (R.stopped) {
+        if (threadIdx.x == 0) {
+            R.go = 0;
+            R.done = 1;
+        }
+        return;
+    }
+    __shared__ double sh[32];
+    __shared__ double dd0[kRedWidth];
+    const int k = R.k, nh = ens_nh(k);
+    for (int m = 0; m <= nh; m++) {
+        double v = 0.0;
+        for (int b = threadIdx.x; b < R.red_blocks; b += blockDim.x) v += R.partials[(long long)b * kRedWidth + m];
+        v = block_sum(v, sh);
+        if (threadIdx.x == 0) dd0[m] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
+    if (lane <= nh) R.DD[0][lane] = dd0[lane];
+    __syncwarp();
+    const double DD00 = dd0[0];
+    bool ok = true;
+    if (k >= 2) {
+        // U_mn = DD00 - DD0m - DD0n + DD_nm (upper triangle), V_m = DD00 - DD0m
+        double a[kMaxHist];
+        const int m = lane + 1;  // this lane's row
+#pragma unroll
+        for (int c = 0; c < kMaxHist; c++) {
+            const int n = c + 1;
+            a[c] = 0.0;
+            if (m <= nh && n <= nh) {
+                const int lo = m < n ? m : n, hi = m < n ? n : m;
+                a[c] = __dadd_rn(__dsub_rn(__dsub_rn(DD00, dd0[hi]), dd0[lo]), R.DD[lo][hi]);
+            }
+        }
+        const double v = m <= nh ? __dsub_rn(DD00, dd0[m]) : 0.0;
+        double x = 0.0;
+        ok = lu_solve_warp(a, v, x, nh);
+        if (ok && lane < nh) R.coef[lane] = x;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        R.simple = k < 2;
+        if (!ok) {
+            R.singular = 1;
+            R.stopped = 1;
+            R.go = 0;
+        } else {
+            R.go = 1;
+            // the current deviation becomes history slot n (src/anderson.cc:82-89)
+            const int n = 1 + (k - 1) % kMaxHist;
+            R.DD[n][n] = DD00;
+            for (int c = 1; c < n; c++) R.DD[c][n] = dd0[c];
+            for (int c = n + 1; c <= nh; c++) R.DD[n][c] = dd0[c];
+            // err = (S1/M)^(1/2) (the reference takes pow(., 0.5); sqrt is the
+            // correctly rounded value of the same)
+            const double err = sqrt(__ddiv_rn(DD00, (double)R.M));
+            if (!(err > tol) || !(k + 1 < maxIter)) R.stopped = 1;
+        }
+    }
+}
+
+// w+ update (src/anderson.cc:57-79): grid (max red_blocks, nrep); lambda[k] =
+// 1 - 0.9^k from the host
+__global__ void __launch_bounds__(256) ens_update_kernel(EnsRep *__restrict__ reps, const double *__restrict__ lambda)
+{
+    const EnsRep &R = reps[blockIdx.y];
+    if (!R.active || !R.go || (int)blockIdx.x >= R.red_blocks) return;
+    const int nh = ens_nh(R.k);
+    HistPtrs Dhp{}, whp{};
+    for (int m = 1; m <= nh; m++) {
+        Dhp.p[m - 1] = R.Dh[R.phys[m]];
+        whp.p[m - 1] = R.wh[R.phys[m]];
+    }
+    anderson_update_body(R.w + R.M, R.wh[R.cur], R.Dh[R.cur], R.M, lambda[R.k], nh, R.simple, Dhp, whp, R.coef,
+                         blockIdx.x, R.red_blocks);
+}
+
+// After each body iteration: history rotation (src/anderson.cc:82-89) and
+// the next iteration number of every active replica; replicas whose extra
+// iteration just ran become idle.  Ends the WHILE loop when none is active.
+__global__ void ens_control_kernel(EnsRep *__restrict__ reps, int nrep, cudaGraphConditionalHandle loop)
+{
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    for (int r = threadIdx.x; r < nrep; r += blockDim.x) {
+        EnsRep &R = reps[r];
+        if (!R.active) continue;
+        if (R.done) {
+            R.active = 0;
+            R.iters = R.k;
+            continue;
+        }
+        if (R.go) {
+            const int n = 1 + (R.k - 1) % kMaxHist;
+            const int evicted = R.phys[n];
+            R.phys[n] = R.cur;
+            R.cur = evicted;
+        }
+        R.k++;
+        any = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) cudaGraphSetConditional(loop, any ? 1u : 0u);
+}
+
+// start of a mix: every replica active at iteration 1; with advance, the
+// Langevin step counter moves on (after this step's update used it)
+__global__ void ens_begin_kernel(EnsRep *__restrict__ reps, int nrep, long long *step, int advance)
+{
+    for (int r = threadIdx.x; r < nrep; r += blockDim.x) {
+        EnsRep &R = reps[r];
+        R.k = 1;
+        R.active = 1;
+        R.stopped = R.done = R.go = R.singular = 0;
+    }
+    if (advance && threadIdx.x == 0) *step += 1;
+}
+
+// W- += -(phi- + 2 W-/XbN) dt + (eta_prev + eta_new)/2 (src/langevin.cc:31),
+// the noise of steps s-1 and s regenerated from the counter: grid (blocks, nrep)
+__global__ void __launch_bounds__(256) ens_langevin_kernel(EnsRep *__restrict__ reps, const long long *step)
+{
+    const EnsRep &R = reps[blockIdx.y];
+    const long long s = *step;
+    double *w = R.w;
+    const long long M = R.M;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < M; r += stride) {
+        const double ep = philox_noise(R.seed, s - 1, r, R.sigma);
+        const double en = philox_noise(R.seed, s, r, R.sigma);
+        const double wm = w[r], pm = w[2 * M + r];
+        const double drift = __dmul_rn(-__dadd_rn(pm, __ddiv_rn(__dmul_rn(2.0, wm), R.XbN)), R.dt);
+        const double noise = __dmul_rn(0.5, __dadd_rn(ep, en));
+        w[r] = __dadd_rn(wm, __dadd_rn(drift, noise));
+    }
+}
+
+// the noise sigma * z of points [0, n) of step s (for callers that feed it to
+// a single context, and for tests)
+__global__ void philox_noise_kernel(unsigned long long seed, long long s, long long n, double sigma, double *out)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride)
+        out[r] = philox_noise(seed, s, r, sigma);
+}
+
+}  // namespace lfts

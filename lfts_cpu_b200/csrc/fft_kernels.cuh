@@ -676,8 +676,10 @@ struct PencilCfg {
     static __device__ __forceinline__ int row(int r) { return SWZ ? (r ^ ((r / R2) & 1)) : r; }
 };
 
+// body of one CTA: column tile `tile` of chain `chain` (the ensemble's
+// batched launches call it with their own tile numbering)
 template <typename T, int NX, int CW, int MODE>
-__global__ void __launch_bounds__(PencilCfg<T, NX, CW>::NT) pencil_kernel(PencilArgs<T> a)
+__device__ __forceinline__ void pencil_body(const PencilArgs<T> &a, const int tile, const int chain)
 {
     using C = PencilCfg<T, NX, CW>;
     constexpr int R1 = C::R1, R2 = C::R2;
@@ -686,7 +688,7 @@ __global__ void __launch_bounds__(PencilCfg<T, NX, CW>::NT) pencil_kernel(Pencil
     cpx<T> *twx = Tl + NX * CW;
     T *gxs = reinterpret_cast<T *>(twx + NX);
 
-    const int col0 = blockIdx.x * CW, c = blockIdx.y + a.cbase;
+    const int col0 = tile * CW, c = chain + a.cbase;
     const int ncol = a.ncol;
     cpx<T> *Sg = a.spec + (long long)c * NX * ncol;
     for (int t = threadIdx.x; t < NX; t += C::NT) {
@@ -755,6 +757,12 @@ __global__ void __launch_bounds__(PencilCfg<T, NX, CW>::NT) pencil_kernel(Pencil
 #pragma unroll
         for (int j1 = 0; j1 < R1; j1++) Sg[(long long)(j2 + R2 * j1) * ncol + col] = v[j1];
     }
+}
+
+template <typename T, int NX, int CW, int MODE>
+__global__ void __launch_bounds__(PencilCfg<T, NX, CW>::NT) pencil_kernel(PencilArgs<T> a)
+{
+    pencil_body<T, NX, CW, MODE>(a, blockIdx.x, blockIdx.y);
 }
 
 }  // namespace lfts

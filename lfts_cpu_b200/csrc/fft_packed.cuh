@@ -291,8 +291,10 @@ struct PcTw {
     }
 };
 
+// body of one CTA: x-plane x of an mx-plane field (the ensemble's batched
+// launches call it with their own plane numbering)
 template <typename T, int NY, int NZ, int MODE>
-__global__ void __launch_bounds__(PlaneCCfg<T, NY, NZ>::NT, 1) plane_c_kernel(PlaneArgs<T> a)
+__device__ __forceinline__ void plane_c_body(const PlaneArgs<T> &a, const int x, const int mx)
 {
     using C = PlaneCCfg<T, NY, NZ>;
     constexpr int KP = C::KP;
@@ -302,8 +304,6 @@ __global__ void __launch_bounds__(PlaneCCfg<T, NY, NZ>::NT, 1) plane_c_kernel(Pl
     cpx<T> *twa = twy + NY;
     cpx<T> *twb = twa + C::NTA;
 
-    const int x = blockIdx.x;
-    const int mx = gridDim.x;
     const long long M = (long long)mx * NY * NZ;
     const long long plane_off = (long long)x * NY * NZ;
     cpx<T> *Sg = a.spec + (long long)x * NY * NZ;
@@ -395,6 +395,12 @@ __global__ void __launch_bounds__(PlaneCCfg<T, NY, NZ>::NT, 1) plane_c_kernel(Pl
     pc_y_B<C, -1, true>(P, twy);
     __syncthreads();
     pc_y_fwdA_global<C>(P, Sg);
+}
+
+template <typename T, int NY, int NZ, int MODE>
+__global__ void __launch_bounds__(PlaneCCfg<T, NY, NZ>::NT, 1) plane_c_kernel(PlaneArgs<T> a)
+{
+    plane_c_body<T, NY, NZ, MODE>(a, blockIdx.x, gridDim.x);
 }
 
 }  // namespace lfts

@@ -38,7 +38,7 @@ __device__ __forceinline__ double block_sum(double v, double *sh)
 }
 
 // Q = sum(qpart)/M and ln Q (src/diblock.cc:46-48,59)
-__global__ void q_finalize_kernel(const double *qpart, int n, long long M, double *Q_out)
+static __global__ void q_finalize_kernel(const double *qpart, int n, long long M, double *Q_out)
 {
     __shared__ double sh[32];
     double s = 0.0;
@@ -70,11 +70,15 @@ __device__ __forceinline__ void vload(const T *p, T (&out)[V])
 // Anderson residual Dh0 = phi+ - 1 with partial sums of Dh0*Dh0 and
 // Dh0*Dh_m, m = 1..nh (src/anderson.cc:35-55).  Each thread handles V
 // consecutive mesh points with vector loads; h comes from slot 1 (= [hA|hB]).
+// body of block `blk` of `nblk` (the grid-stride partition fixes the order of
+// the dot-product partial sums, so a replica's result does not depend on how
+// its blocks are launched)
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads, 4) concentrations_kernel(
+__device__ __forceinline__ void concentrations_body(
     const T *__restrict__ q, long long M, int N, int NA, const double *__restrict__ w,
     double *__restrict__ phim, double *__restrict__ phip, const double *__restrict__ Qd,
-    double *__restrict__ Dh0, int nh, HistPtrs hist, double *__restrict__ partials)
+    double *__restrict__ Dh0, int nh, const HistPtrs &hist, double *__restrict__ partials, const int blk,
+    const int nblk)
 {
     constexpr int V = sizeof(T) == 4 ? 4 : 2;
     __shared__ double sh[kRedThreads / 32];
@@ -84,8 +88,8 @@ __global__ void __launch_bounds__(kRedThreads, 4) concentrations_kernel(
 #pragma unroll
     for (int m = 0; m < kRedWidth; m++) acc[m] = 0.0;
     const long long nvec = M / V;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < nvec; g += stride) {
+    const long long stride = (long long)nblk * blockDim.x;
+    for (long long g = (long long)blk * blockDim.x + threadIdx.x; g < nvec; g += stride) {
         const long long r0 = g * V;
         // slot i holds [q_i | q^_{N+1-i}] (src/diblock.cc:19-24); slot i at q + (i-1)*2M
         double sA[V], sB[V];
@@ -148,12 +152,21 @@ __global__ void __launch_bounds__(kRedThreads, 4) concentrations_kernel(
     for (int m = 0; m < kRedWidth; m++) {
         if (m > nh) break;
         const double s = block_sum(acc[m], sh);
-        if (threadIdx.x == 0) partials[(long long)blockIdx.x * kRedWidth + m] = s;
+        if (threadIdx.x == 0) partials[(long long)blk * kRedWidth + m] = s;
     }
 }
 
+template <typename T>
+static __global__ void __launch_bounds__(kRedThreads, 4) concentrations_kernel(
+    const T *__restrict__ q, long long M, int N, int NA, const double *__restrict__ w,
+    double *__restrict__ phim, double *__restrict__ phip, const double *__restrict__ Qd,
+    double *__restrict__ Dh0, int nh, HistPtrs hist, double *__restrict__ partials)
+{
+    concentrations_body<T>(q, M, N, NA, w, phim, phip, Qd, Dh0, nh, hist, partials, blockIdx.x, gridDim.x);
+}
+
 // out[m] = sum over blocks of partials[b][m], m < width, fixed order
-__global__ void reduce_partials_kernel(const double *partials, int nblocks, int width, double *out)
+static __global__ void reduce_partials_kernel(const double *partials, int nblocks, int width, double *out)
 {
     __shared__ double sh[32];
     for (int m = 0; m < width; m++) {
@@ -166,13 +179,13 @@ __global__ void reduce_partials_kernel(const double *partials, int nblocks, int 
 
 // w+ update of one Anderson iteration (src/anderson.cc:57-79) and the copy
 // of the pre-update w+ into the current history slot (wh_[0], :38).
-__global__ void anderson_update_kernel(double *__restrict__ wp, double *__restrict__ wh0,
-                                       const double *__restrict__ Dh0, long long M, double lambda,
-                                       int nh, int simple, HistPtrs Dh, HistPtrs wh, Coefs C)
+__device__ __forceinline__ void anderson_update_body(double *__restrict__ wp, double *__restrict__ wh0,
+                                                     const double *__restrict__ Dh0, long long M, double lambda,
+                                                     int nh, int simple, const HistPtrs &Dh, const HistPtrs &wh,
+                                                     const double *c, const int blk, const int nblk)
 {
-    const double *c = C.c;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < M; r += stride) {
+    const long long stride = (long long)nblk * blockDim.x;
+    for (long long r = (long long)blk * blockDim.x + threadIdx.x; r < M; r += stride) {
         const double old = wp[r];
         const double d0 = Dh0[r];
         wh0[r] = old;
@@ -191,8 +204,15 @@ __global__ void anderson_update_kernel(double *__restrict__ wp, double *__restri
     }
 }
 
+static __global__ void anderson_update_kernel(double *__restrict__ wp, double *__restrict__ wh0,
+                                       const double *__restrict__ Dh0, long long M, double lambda,
+                                       int nh, int simple, HistPtrs Dh, HistPtrs wh, Coefs C)
+{
+    anderson_update_body(wp, wh0, Dh0, M, lambda, nh, simple, Dh, wh, C.c, blockIdx.x, gridDim.x);
+}
+
 // W- += -(phi- + 2 W-/XbN) dt + (eta_prev + eta_new)/2   (src/langevin.cc:31)
-__global__ void langevin_kernel(double *__restrict__ w, long long M, const double *__restrict__ eta_prev,
+static __global__ void langevin_kernel(double *__restrict__ w, long long M, const double *__restrict__ eta_prev,
                                 const double *__restrict__ eta_new, double XbN, double dt)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -205,7 +225,7 @@ __global__ void langevin_kernel(double *__restrict__ w, long long M, const doubl
 }
 
 // partial sums of w+ and W-^2 (src/lfts_simulation.cc:129-131)
-__global__ void __launch_bounds__(kRedThreads) h_sums_kernel(const double *__restrict__ w, long long M,
+static __global__ void __launch_bounds__(kRedThreads) h_sums_kernel(const double *__restrict__ w, long long M,
                                                              double *partials)
 {
     __shared__ double sh[kRedThreads / 32];
@@ -224,7 +244,7 @@ __global__ void __launch_bounds__(kRedThreads) h_sums_kernel(const double *__res
 
 // Spherical average of S(k) (src/strFunc.cc:50-76): one thread per |K| bin,
 // summing its wavevectors in the reference's stable-sorted order.
-__global__ void sk_bin_kernel(const double *__restrict__ S, const int *__restrict__ order,
+static __global__ void sk_bin_kernel(const double *__restrict__ S, const int *__restrict__ order,
                               const int *__restrict__ wt, const int *__restrict__ bin_start, int nbins,
                               double coeff_over_ns, double half_over_chi, double *__restrict__ out)
 {
@@ -242,7 +262,7 @@ __global__ void sk_bin_kernel(const double *__restrict__ S, const int *__restric
 }
 
 template <typename Tin, typename Tout>
-__global__ void convert_kernel(const Tin *__restrict__ in, Tout *__restrict__ out, long long n)
+static __global__ void convert_kernel(const Tin *__restrict__ in, Tout *__restrict__ out, long long n)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/lfts_b200.h"
+#include "ctx.h"
 #include "fft_dispatch.h"
 #include "field_kernels.cuh"
 
@@ -101,74 +102,6 @@ inline int signed_k(int K, int m) { return (K <= m / 2) ? K : K - m; }
 // shared with lfts_noalloc.cu, which reports through lfts_last_error_string
 void lfts_internal_set_error(const char *msg) { g_last_error = msg; }
 
-struct lfts_ctx {
-    lfts_params p{};
-    int prec = 0, dev = 0;
-    int N = 0, NA = 0, NB = 0;
-    int mx = 0, my = 0, mz = 0, KZ = 0;
-    long long M = 0, Mk = 0;
-    size_t tsize = 8;  // bytes of the propagator type
-    cudaStream_t st = nullptr;
-    cudaStream_t st1 = nullptr;         // chain 1 of the contour chain runs here
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    int sms = 148;
-
-    double *w = nullptr;       // 4M: W-, w+, phi-, phi+
-    void *q = nullptr;         // N slots x 2M, slot i at (i-1)*2M
-    void *spec = nullptr;      // 2 x mx x my x KZ complex
-    void *tw[3] = {};          // exp(-2 pi i t/m) per dimension
-    void *gtab[3] = {};        // gx[mx], gy[my], gz[KZ] (gz carries 1/M)
-    double *qpart = nullptr;   // mx per-plane sums of q_N
-    double *Qd = nullptr;      // Q, ln Q
-    double *partials = nullptr;
-    double *red = nullptr;     // kRedWidth reduced values (device)
-    double *red_host = nullptr;  // pinned copy
-    int red_blocks = 0;
-
-    double *eta[2] = {};       // Langevin noise: prev, new
-    int eta_prev = 0;
-    bool eta_set = false;
-
-    double *Dh[kRedWidth] = {}, *wh[kRedWidth] = {};  // Anderson ring (physical buffers)
-    int phys[kRedWidth] = {};  // logical history slot -> physical buffer
-    int cur = 0;               // physical buffer of the current iteration
-    double DD[kRedWidth][kRedWidth] = {};
-
-    double *S = nullptr;       // S(k) accumulator (Mk)
-    void *skspec = nullptr;    // FP64 spectrum scratch for S(k)
-    bool sk_own_spec = false;
-    void *sktw[3] = {};        // FP64 twiddles (FP32 contexts only)
-    int nsamples = 0;
-    double sk_dK = -1.0;
-    int sk_nbins = 0;
-    int *sk_order = nullptr, *sk_wt = nullptr, *sk_bins = nullptr;
-    double *sk_out = nullptr;
-    std::vector<double> sk_K;  // K value reported for each bin
-
-    void *sf_buf = nullptr;    // step_fwd scratch: q_in, q_out, h (2M each, FP64)
-    double *adj_partial = nullptr;  // adjoint block partials [blocks][3]
-    double *adj_buf = nullptr;      // checkpointed adjoint: recomputed q segment + discard row
-    int adj_buf_slots = 0;
-    AdjKernel adj{};
-
-    PlaneKernels<double> pl64{};
-    PencilKernels<double> pe64{};
-    PlaneKernels<float> pl32{};
-    PencilKernels<float> pe32{};
-    int plane_stages = 2;     // yz-plane transform stages per axis (3: fft_plane3.cuh)
-
-    bool fields_set = false;
-    bool have_concs = false;
-    bool packed = false;      // FP32: both chains as one complex field (fft_packed.cuh)
-    bool use_graph = true;    // LFTS_NO_GRAPH=1: launch the chain kernel by kernel
-    cudaGraph_t chain_graph = nullptr;
-    cudaGraphExec_t chain_exec = nullptr;
-    long long chain_kernels = 0;  // kernels in one replay of chain_exec
-    bool use_pdl = true;      // LFTS_NO_PDL=1 in the environment turns it off
-    bool two_streams = true;  // LFTS_ONE_STREAM=1 runs both chains in each launch
-    long long launches = 0;
-    long long mix_calls = 0, mix_iters = 0;
-};
 
 namespace {
 

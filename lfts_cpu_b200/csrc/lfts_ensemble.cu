@@ -1,0 +1,507 @@
+// Ensemble of independent FP32-mixed L-FTS replicas advanced together
+// (include/lfts_b200.h, "ensemble").  Each replica is an ordinary context
+// (buffers, tables, autotuned x-pencil width); the ensemble adds batched
+// launches over the replicas of each mesh, the device-side Anderson loop of
+// ensemble_kernels.cuh and on-device Philox noise, and captures one whole
+// Langevin step of every replica as one CUDA graph:
+//
+//   [Langevin update, all replicas] -> [begin] -> WHILE (any replica active) {
+//       per mesh group, on its own stream: INIT_W plane, N-1 x (x-pencil, plane)
+//       -> Q, concentrations + dots, reduction + least squares, w+ update,
+//       control (sets the WHILE condition) }
+//
+// so a step costs one graph launch and no host round trip.
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "ctx.h"
+#include "ensemble_kernels.cuh"
+
+using namespace lfts;
+
+extern void lfts_internal_set_error(const char *msg);
+
+namespace {
+
+#define EK(call)                                                                   \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) {                                                   \
+            std::string m_ = std::string(#call) + ": " + cudaGetErrorString(e_);   \
+            lfts_internal_set_error(m_.c_str());                                   \
+            return LFTS_ERR_CUDA;                                                  \
+        }                                                                          \
+    } while (0)
+
+using PlaneFn = void (*)(EnsRep *, const int *, int);
+using PencilFn = void (*)(EnsRep *, const int *);
+
+struct PlaneSet {
+    PlaneFn fn[4];
+    int nt;
+    size_t smem;
+};
+struct PencilSet {
+    PencilFn fn;
+    int nt;
+    size_t smem;
+};
+
+// meshes (per side) with batched kernels: cubic 16 ... 96
+#define LFTS_ENS_LEN(X) X(16) X(24) X(32) X(48) X(64) X(96)
+
+template <int N>
+void fill_plane(PlaneSet *o)
+{
+    using C = PlaneCCfg<float, N, N>;
+    o->fn[PLANE_INIT_W] = ens_plane_kernel<N, N, PLANE_INIT_W>;
+    o->fn[PLANE_INIT_Q] = ens_plane_kernel<N, N, PLANE_INIT_Q>;
+    o->fn[PLANE_STEP] = ens_plane_kernel<N, N, PLANE_STEP>;
+    o->fn[PLANE_LAST] = ens_plane_kernel<N, N, PLANE_LAST>;
+    o->nt = C::NT;
+    o->smem = C::SMEM;
+}
+
+template <int N, int CW>
+void fill_pencil(PencilSet *o)
+{
+    using C = PencilCfg<float, N, CW>;
+    o->fn = ens_pencil_kernel<N, CW>;
+    o->nt = C::NT;
+    o->smem = C::SMEM;
+}
+
+bool ens_plane(int ny, int nz, PlaneSet *o)
+{
+    if (ny != nz) return false;
+#define X(n)                    \
+    if (ny == n) {              \
+        fill_plane<n>(o);       \
+        return true;            \
+    }
+    LFTS_ENS_LEN(X)
+#undef X
+    return false;
+}
+
+bool ens_pencil(int nx, int cw, PencilSet *o)
+{
+#define X(n)                                                \
+    if (nx == n) {                                          \
+        if (cw == 8) { fill_pencil<n, 8>(o); return true; }   \
+        if (cw == 16) { fill_pencil<n, 16>(o); return true; } \
+        if (cw == 32) { fill_pencil<n, 32>(o); return true; } \
+        return false;                                       \
+    }
+    LFTS_ENS_LEN(X)
+#undef X
+    return false;
+}
+
+struct Group {
+    int mx = 0, my = 0, mz = 0, cw = 0;
+    std::vector<int> members;
+    int *d_members = nullptr;
+    PlaneSet pl{};
+    PencilSet pe{};
+    cudaStream_t st = nullptr;
+    cudaEvent_t join = nullptr;
+};
+
+}  // namespace
+
+struct lfts_ensemble {
+    int dev = 0, nrep = 0, N = 0;
+    std::vector<lfts_ctx *> rep;
+    std::vector<EnsRep> h_reps;
+    EnsRep *d_reps = nullptr;
+    std::vector<Group> groups;
+    cudaStream_t s0 = nullptr;
+    cudaEvent_t fork = nullptr;
+    long long *d_step = nullptr;  // Langevin step counter (next step's index)
+    double *d_lambda = nullptr;   // 1 - 0.9^k, k < lambda_n
+    int lambda_n = 0;
+    int max_blocks = 0;           // largest reduction grid of any replica
+    // graphs, built for one (maxIter, tol)
+    cudaGraph_t g_mix = nullptr, g_step = nullptr;
+    cudaGraphExec_t x_mix = nullptr, x_step = nullptr;
+    int g_maxIter = -1;
+    double g_tol = -1.0;
+    long long launches = 0;
+};
+
+namespace {
+
+struct EnsDeviceGuard {
+    int prev = -1;
+    explicit EnsDeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~EnsDeviceGuard()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+// one iteration of every active replica, enqueued on e->s0 (being captured)
+int enqueue_body(lfts_ensemble *e, int maxIter, double tol, cudaGraphConditionalHandle loop)
+{
+    EK(cudaEventRecord(e->fork, e->s0));
+    for (Group &g : e->groups) {
+        EK(cudaStreamWaitEvent(g.st, e->fork, 0));
+        const int nm = (int)g.members.size();
+        const dim3 pgrid(g.mx, nm);
+        const dim3 egrid((g.my * g.mz + g.cw - 1) / g.cw, nm);
+        g.pl.fn[PLANE_INIT_W]<<<pgrid, g.pl.nt, g.pl.smem, g.st>>>(e->d_reps, g.d_members, 0);
+        e->launches++;
+        for (int i = 1; i < e->N; i++) {
+            g.pe.fn<<<egrid, g.pe.nt, g.pe.smem, g.st>>>(e->d_reps, g.d_members);
+            g.pl.fn[i + 1 < e->N ? PLANE_STEP : PLANE_LAST]<<<pgrid, g.pl.nt, g.pl.smem, g.st>>>(e->d_reps,
+                                                                                               g.d_members, i);
+            e->launches += 2;
+        }
+        EK(cudaGetLastError());
+        EK(cudaEventRecord(g.join, g.st));
+        EK(cudaStreamWaitEvent(e->s0, g.join, 0));
+    }
+    ens_qfinal_kernel<<<e->nrep, 256, 0, e->s0>>>(e->d_reps);
+    ens_conc_kernel<<<dim3(e->max_blocks, e->nrep), kRedThreads, 0, e->s0>>>(e->d_reps);
+    ens_reduce_solve_kernel<<<e->nrep, 256, 0, e->s0>>>(e->d_reps, tol, maxIter);
+    ens_update_kernel<<<dim3(e->max_blocks, e->nrep), 256, 0, e->s0>>>(e->d_reps, e->d_lambda);
+    ens_control_kernel<<<1, 256, 0, e->s0>>>(e->d_reps, e->nrep, loop);
+    e->launches += 5;
+    EK(cudaGetLastError());
+    return LFTS_OK;
+}
+
+// [Langevin update ->] begin -> WHILE(body)
+int build_graph(lfts_ensemble *e, bool langevin, int maxIter, double tol, cudaGraph_t *g_out, cudaGraphExec_t *x_out)
+{
+    cudaGraph_t g = nullptr;
+    EK(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle loop;
+    EK(cudaGraphConditionalHandleCreate(&loop, g, 1, cudaGraphCondAssignDefault));
+
+    // prologue, captured into g
+    EK(cudaStreamBeginCaptureToGraph(e->s0, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    if (langevin) {
+        long long maxM = 0;
+        for (const EnsRep &r : e->h_reps) maxM = std::max(maxM, r.M);
+        const int lb = (int)std::min<long long>((maxM + 255) / 256, 1184);
+        ens_langevin_kernel<<<dim3(lb, e->nrep), 256, 0, e->s0>>>(e->d_reps, e->d_step);
+    }
+    ens_begin_kernel<<<1, 256, 0, e->s0>>>(e->d_reps, e->nrep, e->d_step, langevin ? 1 : 0);
+    cudaGraph_t captured = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(e->s0, &captured);
+    if (ce != cudaSuccess) {
+        cudaGraphDestroy(g);
+        EK(ce);
+    }
+    // the prologue's last node: the one without dependents
+    size_t nn = 0;
+    EK(cudaGraphGetNodes(g, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    EK(cudaGraphGetNodes(g, nodes.data(), &nn));
+    cudaGraphNode_t last = nullptr;
+    for (cudaGraphNode_t n : nodes) {
+        size_t nd = 0;
+        EK(cudaGraphNodeGetDependentNodes(n, nullptr, &nd));
+        if (nd == 0) last = n;
+    }
+
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = loop;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cond = nullptr;
+    EK(cudaGraphAddNode(&cond, g, &last, last ? 1 : 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    EK(cudaStreamBeginCaptureToGraph(e->s0, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_body(e, maxIter, tol, loop);
+    cudaGraph_t body_out = nullptr;
+    ce = cudaStreamEndCapture(e->s0, &body_out);
+    if (rc) {
+        cudaGraphDestroy(g);
+        return rc;
+    }
+    if (ce != cudaSuccess) {
+        cudaGraphDestroy(g);
+        EK(ce);
+    }
+    cudaGraphExec_t x = nullptr;
+    ce = cudaGraphInstantiate(&x, g, 0);
+    if (ce != cudaSuccess) {
+        cudaGraphDestroy(g);
+        EK(ce);
+    }
+    EK(cudaGraphUpload(x, e->s0));
+    EK(cudaStreamSynchronize(e->s0));
+    *g_out = g;
+    *x_out = x;
+    return LFTS_OK;
+}
+
+void drop_graphs(lfts_ensemble *e)
+{
+    if (e->x_mix) cudaGraphExecDestroy(e->x_mix);
+    if (e->x_step) cudaGraphExecDestroy(e->x_step);
+    if (e->g_mix) cudaGraphDestroy(e->g_mix);
+    if (e->g_step) cudaGraphDestroy(e->g_step);
+    e->x_mix = e->x_step = nullptr;
+    e->g_mix = e->g_step = nullptr;
+}
+
+int ensure_graphs(lfts_ensemble *e, int maxIter, double tol)
+{
+    if (e->x_mix && e->g_maxIter == maxIter && e->g_tol == tol) return LFTS_OK;
+    drop_graphs(e);
+    // lambda_k = 1 - 0.9^k (src/anderson.cc:44), host pow as in the single context
+    std::vector<double> lam(maxIter + 2);
+    for (int k = 0; k < (int)lam.size(); k++) lam[k] = 1.0 - std::pow(0.9, double(k));
+    if (e->d_lambda) cudaFree(e->d_lambda);
+    e->d_lambda = nullptr;
+    EK(cudaMalloc(&e->d_lambda, sizeof(double) * lam.size()));
+    EK(cudaMemcpy(e->d_lambda, lam.data(), sizeof(double) * lam.size(), cudaMemcpyHostToDevice));
+    e->lambda_n = (int)lam.size();
+    int rc = build_graph(e, false, maxIter, tol, &e->g_mix, &e->x_mix);
+    if (!rc) rc = build_graph(e, true, maxIter, tol, &e->g_step, &e->x_step);
+    if (rc) {
+        drop_graphs(e);
+        return rc;
+    }
+    e->g_maxIter = maxIter;
+    e->g_tol = tol;
+    return LFTS_OK;
+}
+
+int read_back(lfts_ensemble *e, int *k_out, double *lnQ_out)
+{
+    EK(cudaStreamSynchronize(e->s0));
+    EK(cudaMemcpy(e->h_reps.data(), e->d_reps, sizeof(EnsRep) * e->nrep, cudaMemcpyDeviceToHost));
+    int singular = -1;
+    for (int r = 0; r < e->nrep; r++) {
+        if (k_out) k_out[r] = e->h_reps[r].iters;
+        if (e->h_reps[r].singular && singular < 0) singular = r;
+        if (lnQ_out) EK(cudaMemcpy(&lnQ_out[r], e->h_reps[r].Qd + 1, sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    if (singular >= 0) {
+        lfts_internal_set_error("Anderson least-squares matrix is singular in a replica");
+        return LFTS_ERR_SINGULAR;
+    }
+    return LFTS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lfts_ensemble_create(const lfts_params *params, const unsigned long long *seeds, int nrep, int device,
+                         lfts_ensemble **out)
+{
+    if (!params || !seeds || nrep < 1 || !out) return LFTS_ERR_ARG;
+    *out = nullptr;
+    for (int r = 0; r < nrep; r++) {
+        const lfts_params &p = params[r];
+        if (p.N != params[0].N) {
+            lfts_internal_set_error("ensemble replicas must share the chain length N");
+            return LFTS_ERR_ARG;
+        }
+        PlaneSet ps;
+        PencilSet qs;
+        if (!ens_plane(p.m[1], p.m[2], &ps) || !ens_pencil(p.m[0], 16, &qs)) {
+            lfts_internal_set_error("ensemble meshes: 16, 24, 32, 48, 64 or 96 points per side, cubic planes");
+            return LFTS_ERR_UNSUPPORTED;
+        }
+    }
+    EnsDeviceGuard dg(device);
+    lfts_ensemble *e = new lfts_ensemble();
+    e->dev = device;
+    e->nrep = nrep;
+    e->N = params[0].N;
+    auto fail = [&](int code) {
+        lfts_ensemble_destroy(e);
+        return code;
+    };
+    for (int r = 0; r < nrep; r++) {
+        lfts_ctx *c = nullptr;
+        int rc = lfts_create(&params[r], LFTS_FP32_MIXED, device, &c);
+        if (rc) return fail(rc);
+        e->rep.push_back(c);
+    }
+    e->h_reps.resize(nrep);
+    for (int r = 0; r < nrep; r++) {
+        lfts_ctx *c = e->rep[r];
+        EnsRep &R = e->h_reps[r];
+        std::memset(&R, 0, sizeof(R));
+        R.mx = c->mx;
+        R.my = c->my;
+        R.mz = c->mz;
+        R.N = c->N;
+        R.NA = c->NA;
+        R.NB = c->NB;
+        R.M = c->M;
+        R.red_blocks = c->red_blocks;
+        R.XbN = c->p.XbN;
+        R.dt = c->p.dt;
+        // sigma = sqrt(2 M dt / (C V))  (src/lfts_params.cc:117)
+        const double V = c->p.L[0] * c->p.L[1] * c->p.L[2];
+        R.sigma = std::sqrt(2.0 * (double)c->M * c->p.dt / (c->p.C * V));
+        R.seed = seeds[r];
+        R.w = c->w;
+        R.q = static_cast<float *>(c->q);
+        R.spec = static_cast<cpx<float> *>(c->spec);
+        for (int d = 0; d < 3; d++) {
+            R.tw[d] = static_cast<const cpx<float> *>(c->tw[d]);
+            R.g[d] = static_cast<const float *>(c->gtab[d]);
+        }
+        R.qpart = c->qpart;
+        R.Qd = c->Qd;
+        R.partials = c->partials;
+        for (int i = 0; i < kRedWidth; i++) {
+            R.Dh[i] = c->Dh[i];
+            R.wh[i] = c->wh[i];
+            R.phys[i] = c->phys[i];
+        }
+        R.cur = c->cur;
+        e->max_blocks = std::max(e->max_blocks, c->red_blocks);
+        // group by mesh; the x-pencil width is the context's autotuned one
+        int gi = -1;
+        for (int g = 0; g < (int)e->groups.size(); g++)
+            if (e->groups[g].mx == c->mx && e->groups[g].my == c->my && e->groups[g].mz == c->mz) gi = g;
+        if (gi < 0) {
+            Group g;
+            g.mx = c->mx;
+            g.my = c->my;
+            g.mz = c->mz;
+            g.cw = c->pe32.cw;
+            ens_plane(g.my, g.mz, &g.pl);
+            if (!ens_pencil(g.mx, g.cw, &g.pe)) return fail(LFTS_ERR_UNSUPPORTED);
+            e->groups.push_back(g);
+            gi = (int)e->groups.size() - 1;
+        }
+        e->groups[gi].members.push_back(r);
+    }
+    if (cudaStreamCreateWithFlags(&e->s0, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess)
+        return fail(LFTS_ERR_CUDA);
+    for (Group &g : e->groups) {
+        if (cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&g.join, cudaEventDisableTiming) != cudaSuccess ||
+            cudaMalloc(&g.d_members, sizeof(int) * g.members.size()) != cudaSuccess ||
+            cudaMemcpy(g.d_members, g.members.data(), sizeof(int) * g.members.size(), cudaMemcpyHostToDevice) !=
+                cudaSuccess)
+            return fail(LFTS_ERR_CUDA);
+        for (int m = 0; m < 4; m++)
+            if (cudaFuncSetAttribute(g.pl.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.pl.smem) !=
+                cudaSuccess)
+                return fail(LFTS_ERR_CUDA);
+        if (cudaFuncSetAttribute(g.pe.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.pe.smem) !=
+            cudaSuccess)
+            return fail(LFTS_ERR_CUDA);
+    }
+    const long long step1 = 1;  // step 0 is the initial noise (the langevin constructor's draw)
+    if (cudaMalloc(&e->d_reps, sizeof(EnsRep) * nrep) != cudaSuccess ||
+        cudaMemcpy(e->d_reps, e->h_reps.data(), sizeof(EnsRep) * nrep, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMalloc(&e->d_step, sizeof(long long)) != cudaSuccess ||
+        cudaMemcpy(e->d_step, &step1, sizeof(long long), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(LFTS_ERR_NOMEM);
+    *out = e;
+    return LFTS_OK;
+}
+
+int lfts_ensemble_destroy(lfts_ensemble *e)
+{
+    if (!e) return LFTS_OK;
+    EnsDeviceGuard dg(e->dev);
+    if (e->s0) cudaStreamSynchronize(e->s0);
+    drop_graphs(e);
+    for (Group &g : e->groups) {
+        if (g.st) cudaStreamDestroy(g.st);
+        if (g.join) cudaEventDestroy(g.join);
+        cudaFree(g.d_members);
+    }
+    if (e->s0) cudaStreamDestroy(e->s0);
+    if (e->fork) cudaEventDestroy(e->fork);
+    cudaFree(e->d_reps);
+    cudaFree(e->d_step);
+    cudaFree(e->d_lambda);
+    for (lfts_ctx *c : e->rep) lfts_destroy(c);
+    delete e;
+    return LFTS_OK;
+}
+
+int lfts_ensemble_set_fields(lfts_ensemble *e, int r, const double *w_host)
+{
+    if (!e || r < 0 || r >= e->nrep || !w_host) return LFTS_ERR_ARG;
+    EnsDeviceGuard dg(e->dev);
+    EK(cudaStreamSynchronize(e->s0));
+    return lfts_set_fields(e->rep[r], w_host);
+}
+
+int lfts_ensemble_get_fields(lfts_ensemble *e, int r, double *w_host)
+{
+    if (!e || r < 0 || r >= e->nrep || !w_host) return LFTS_ERR_ARG;
+    EnsDeviceGuard dg(e->dev);
+    EK(cudaStreamSynchronize(e->s0));
+    return lfts_get_fields(e->rep[r], w_host);
+}
+
+int lfts_ensemble_mix(lfts_ensemble *e, int maxIter, double tol, int *k_out, double *lnQ_out)
+{
+    if (!e || maxIter < 2) return LFTS_ERR_ARG;
+    EnsDeviceGuard dg(e->dev);
+    int rc = ensure_graphs(e, maxIter, tol);
+    if (rc) return rc;
+    EK(cudaGraphLaunch(e->x_mix, e->s0));
+    return read_back(e, k_out, lnQ_out);
+}
+
+int lfts_ensemble_run(lfts_ensemble *e, int nsteps, int maxIter, double tol, int *k_out, double *lnQ_out)
+{
+    if (!e || nsteps < 0 || maxIter < 2) return LFTS_ERR_ARG;
+    EnsDeviceGuard dg(e->dev);
+    int rc = ensure_graphs(e, maxIter, tol);
+    if (rc) return rc;
+    for (int s = 0; s < nsteps; s++) {
+        EK(cudaGraphLaunch(e->x_step, e->s0));
+        if (k_out) {
+            rc = read_back(e, k_out + (long long)s * e->nrep, nullptr);
+            if (rc) return rc;
+        }
+    }
+    return read_back(e, nullptr, lnQ_out);
+}
+
+int lfts_ensemble_tuning(const lfts_ensemble *e, int r, int *pencil_cw)
+{
+    if (!e || r < 0 || r >= e->nrep) return LFTS_ERR_ARG;
+    if (pencil_cw) *pencil_cw = e->rep[r]->pe32.cw;
+    return LFTS_OK;
+}
+
+void *lfts_ensemble_stream(lfts_ensemble *e) { return e ? (void *)e->s0 : nullptr; }
+
+long long lfts_ensemble_kernel_launches(const lfts_ensemble *e) { return e ? e->launches : 0; }
+
+int lfts_noise_philox(unsigned long long seed, long long step, long long n, double sigma, double *out_host)
+{
+    if (!out_host || n < 0) return LFTS_ERR_ARG;
+    if (n == 0) return LFTS_OK;
+    double *d = nullptr;
+    EK(cudaMalloc(&d, sizeof(double) * n));
+    philox_noise_kernel<<<(int)std::min<long long>((n + 255) / 256, 4096), 256>>>(seed, step, n, sigma, d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(out_host, d, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    EK(e);
+    return LFTS_OK;
+}
+
+}  // extern "C"

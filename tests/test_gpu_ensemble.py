@@ -1,0 +1,110 @@
+"""Replica ensemble (lfts_ensemble_*): on-device Philox noise against its
+restatement; every replica of a mixed-mesh ensemble equals a single
+FP32-mixed context fed the same noise (Anderson counts per step, fields,
+ln Q); a run shaped like the batched configuration (32 replicas, meshes
+32/48/64/96, L = mesh/16, N = 64, NA in [16, 48], XN in [12, 20], C = 50)."""
+import numpy as np
+import pytest
+
+import philox_ref
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def lfts(native_lib):
+    import lfts_cpu_b200
+    return lfts_cpu_b200
+
+
+@pytest.mark.parametrize("seed,step,n", [(1, 0, 1001), (0xDEADBEEF12345, 7, 65536), (2**63 + 5, 2**33 + 1, 4096)])
+def test_device_noise_matches_restatement(lfts, seed, step, n):
+    dev = lfts.noise_philox(seed, step, n, 0.37)
+    ref = philox_ref.noise(seed, step, n, 0.37)
+    assert np.max(np.abs(dev - ref)) < 1e-12
+
+
+def replicas_small():
+    return [
+        dict(N=12, NA=5, XbN=13.0, C=50.0, dt=0.5, m=(16, 16, 16), L=(3.0, 3.0, 3.0), seed=11),
+        dict(N=12, NA=7, XbN=15.5, C=80.0, dt=0.4, m=(24, 24, 24), L=(3.6, 3.6, 3.6), seed=12),
+        dict(N=12, NA=4, XbN=12.0, C=50.0, dt=0.5, m=(32, 32, 32), L=(4.0, 4.0, 4.0), seed=13),
+        dict(N=12, NA=6, XbN=17.0, C=50.0, dt=0.5, m=(16, 16, 16), L=(2.5, 2.5, 2.5), seed=14),
+    ]
+
+
+def single_run(lfts, d, w2, nsteps):
+    s = lfts.System(d["N"], d["NA"], d["XbN"], d["C"], d["dt"], d["m"], d["L"], precision=lfts.LFTS_FP32_MIXED)
+    M = int(np.prod(d["m"]))
+    sigma = float(np.sqrt(2.0 * M * d["dt"] / (d["C"] * np.prod(d["L"]))))
+    s.set_fields(w2)
+    k0 = s.mix()
+    lnq0 = s.calc_concs()
+    w0 = s.get_fields()
+    s.langevin_init(lfts.noise_philox(d["seed"], 0, M, sigma))
+    ks = []
+    for st in range(1, nsteps + 1):
+        s.langevin_step(lfts.noise_philox(d["seed"], st, M, sigma))
+        ks.append(s.mix())
+        lnq = s.calc_concs()
+    w = s.get_fields()
+    s.close()
+    return k0, lnq0, w0, ks, lnq, w
+
+
+def test_replicas_equal_single_contexts(lfts):
+    reps = replicas_small()
+    rng = np.random.default_rng(5)
+    fields = [rng.normal(0.0, 1.0, 2 * int(np.prod(d["m"]))) for d in reps]
+    e = lfts.Ensemble(reps)
+    for r, w2 in enumerate(fields):
+        e.set_fields(r, w2)
+    k0, lnq0 = e.mix()
+    w0 = [e.get_fields(r) for r in range(len(reps))]
+    nsteps = 3
+    ks, lnq = e.run(nsteps)
+    w = [e.get_fields(r) for r in range(len(reps))]
+    e.close()
+    for r, d in enumerate(reps):
+        sk0, slnq0, sw0, sks, slnq, sw = single_run(lfts, d, fields[r], nsteps)
+        assert k0[r] == sk0
+        assert lnq0[r] == slnq0
+        assert np.array_equal(w0[r], sw0)
+        assert list(ks[:, r]) == sks
+        assert lnq[r] == slnq
+        assert np.array_equal(w[r], sw)
+
+
+def test_batched_configuration_shape(lfts):
+    """32 replicas drawn from seed like the batched configuration; two steps;
+    discrete-chain identities per replica and one replica of each mesh
+    against its single context."""
+    rng = np.random.default_rng(2024)
+    meshes = rng.choice([32, 48, 64, 96], size=32)
+    reps = []
+    for r, mm in enumerate(meshes):
+        reps.append(dict(N=64, NA=int(rng.integers(16, 49)), XbN=float(rng.uniform(12.0, 20.0)), C=50.0, dt=0.5,
+                         m=(int(mm),) * 3, L=(mm / 16.0,) * 3, seed=1000 + r))
+    fields = [rng.normal(0.0, 0.01, 2 * int(mm) ** 3) for mm in meshes]
+    e = lfts.Ensemble(reps)
+    for r, w2 in enumerate(fields):
+        e.set_fields(r, w2)
+    k0, _ = e.mix()
+    ks, lnq = e.run(2)
+    assert all(e.tuning(r) in (8, 16, 32) for r in range(32))
+    for r, d in enumerate(reps):
+        w = e.get_fields(r)
+        M = int(np.prod(d["m"]))
+        assert np.all(np.isfinite(w))
+        assert abs(w[3 * M:].mean() - 1.0) < 1e-5
+        assert abs(w[2 * M:3 * M].mean() - (2 * d["NA"] - d["N"]) / d["N"]) < 1e-5
+    checked = set()
+    for r, mm in enumerate(meshes):
+        if mm in checked:
+            continue
+        checked.add(mm)
+        sk0, _, _, sks, slnq, sw = single_run(lfts, reps[r], fields[r], 2)
+        assert k0[r] == sk0 and list(ks[:, r]) == sks
+        assert lnq[r] == slnq
+        assert np.array_equal(e.get_fields(r), sw)
+    e.close()
