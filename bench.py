@@ -208,6 +208,85 @@ def run_precision(lfts, precision, steps, warmup, rank, device, torch, clocks=No
     return res
 
 
+def ensemble_config(seed=2024, nrep=32):
+    """The batched configuration: nrep replicas, meshes drawn from seed among
+    32^3, 48^3, 64^3, 96^3, L = mesh/16, N=64, NA in [16,48], XN in [12,20],
+    C=50, Ndt=0.5, separate Philox streams, disordered start (sd 0.01)."""
+    rng = np.random.default_rng(seed)
+    meshes = rng.choice([32, 48, 64, 96], size=nrep)
+    reps = [dict(N=64, NA=int(rng.integers(16, 49)), XbN=float(rng.uniform(12.0, 20.0)), C=50.0, dt=0.5,
+                 m=(int(mm),) * 3, L=(mm / 16.0,) * 3, seed=1000 + r) for r, mm in enumerate(meshes)]
+    fields = [rng.normal(0.0, 0.01, 2 * int(mm) ** 3) for mm in meshes]
+    return reps, fields
+
+
+def ensemble_bench(lfts, torch, device, steps=5, warmup=3):
+    """Replica-steps/s of the batched configuration: one graph launch per
+    Langevin step of all replicas, CUDA events on the ensemble's stream."""
+    reps, fields = ensemble_config()
+    e = lfts.Ensemble(reps, device=device)
+    for r, w2 in enumerate(fields):
+        e.set_fields(r, w2)
+    e.mix(CFG["max_iter"], CFG["tol"])
+    ks, _ = e.run(warmup, CFG["max_iter"], CFG["tol"], record_k=True)
+    stream = torch.cuda.ExternalStream(e.stream(), device=f"cuda:{device}")
+    torch.cuda.synchronize(device)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    e.run(steps, CFG["max_iter"], CFG["tol"], record_k=False)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
+    K = ks.astype(float) - 1.0  # mix returns iterations + 1
+    N = reps[0]["N"]
+    point_steps = sum(float(np.prod(d["m"])) * (N - 1) * (K[:, r].mean() + 1.0) for r, d in enumerate(reps))
+    seq_ms = sequential_single_contexts(lfts, torch, device, reps, fields)
+    out = {"replicas": len(reps), "meshes": {str(mm): int(sum(1 for d in reps if d["m"][0] == mm))
+                                             for mm in (32, 48, 64, 96)},
+           "ms_per_step": ms, "replica_steps_per_s": len(reps) * 1e3 / ms,
+           "mean_anderson_K": float(K.mean()),
+           "mesh_point_contour_steps_per_s": point_steps * 1e3 / ms,
+           "pencil_cw": {str(d["m"][0]): e.tuning(r) for r, d in enumerate(reps)},
+           "timing": f"{steps} steps after {warmup} warm-up steps, one CUDA graph launch per step",
+           "sequential_single_contexts_ms_per_step": seq_ms,
+           "speedup_vs_sequential_single_contexts": seq_ms / ms}
+    e.close()
+    return out
+
+
+def sequential_single_contexts(lfts, torch, device, reps, fields):
+    """The same replicas one after another as single FP32-mixed contexts: sum
+    over replicas of one Langevin step (after the mix and two warm-up
+    steps), CUDA events on each context's stream, same Philox noise."""
+    total = 0.0
+    for d, w2 in zip(reps, fields):
+        M = int(np.prod(d["m"]))
+        sigma = float(np.sqrt(2.0 * M * d["dt"] / (d["C"] * np.prod(d["L"]))))
+        s = lfts.System(d["N"], d["NA"], d["XbN"], d["C"], d["dt"], d["m"], d["L"],
+                        precision=lfts.LFTS_FP32_MIXED, device=device)
+        s.set_fields(w2)
+        s.mix(CFG["max_iter"], CFG["tol"])
+        s.calc_concs()
+        s.langevin_init(lfts.noise_philox(d["seed"], 0, M, sigma))
+        noise = torch.from_numpy(np.stack([lfts.noise_philox(d["seed"], st, M, sigma) for st in (1, 2, 3)]))
+        noise = noise.to(f"cuda:{device}")
+        stream = torch.cuda.ExternalStream(s.stream, device=f"cuda:{device}")
+        for i in range(2):
+            s.full_step_device(noise[i].data_ptr(), CFG["max_iter"], CFG["tol"])
+        torch.cuda.synchronize(device)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        s.full_step_device(noise[2].data_ptr(), CFG["max_iter"], CFG["tol"])
+        ev1.record(stream)
+        ev1.synchronize()
+        total += ev0.elapsed_time(ev1)
+        del noise
+        s.close()
+    return total
+
+
 def barrier(torch):
     import torch.distributed as dist
     if dist.is_available() and dist.is_initialized():
@@ -274,6 +353,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     args = ap.parse_args(argv)
     rank, world, local = dist_env()
     if args.impl == "reference":
@@ -327,6 +407,12 @@ def main(argv=None):
             except Exception as e:  # reported, not fatal
                 cpu = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
                        "sample": f"failed: {e}"}
+        ens = None
+        if not args.no_ensemble and world == 1:
+            try:
+                ens = ensemble_bench(lfts, torch, device)
+            except Exception as e:  # reported, not fatal
+                ens = {"failed": str(e)}
         traffic = None
         tp = os.path.join(ROOT, "profiles", "contour_step_traffic.json")
         if os.path.exists(tp):
@@ -349,12 +435,14 @@ def main(argv=None):
             "gpu_launches": fp32["launches"],
             "mean_anderson_K": K_mean,
             "calc_concs_per_s": fp32["calc_concs_per_step"] * 1e3 / ms32,
+            "mesh_point_contour_steps_per_s": fp32["calc_concs_per_step"] * M * (N - 1) * 1e3 / ms32,
             "hbm_gbs_algorithmic_step": step_alg / (ms32 * 1e-3) / 1e9,
             "fp64": {"value": world * 1e3 / ms64, "ms_per_step": ms64, "mean_anderson_K": float(np.mean(fp64["K"])),
                      "ms_plane": fp64["profile"][0], "ms_pencil": fp64["profile"][1],
                      "calc_concs_per_s": fp64["calc_concs_per_step"] * 1e3 / ms64},
             "speedup_fp32_mixed_vs_fp64": ms64 / ms32,
             "fp32_phi_rel_err_vs_fp64": err_phi, "fp32_lnQ_abs_err_vs_fp64": err_lnq,
+            "ensemble": ens,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
