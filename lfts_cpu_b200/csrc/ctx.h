@@ -40,7 +40,7 @@ struct lfts_ctx {
     int eta_prev = 0;
     bool eta_set = false;
 
-    double *Dh[kRedWidth] = {}, *wh[kRedWidth] = {};  // Anderson ring (physical buffers)
+    void *Dh[kRedWidth] = {}, *wh[kRedWidth] = {};  // Anderson ring (physical buffers, propagator type)
     int phys[kRedWidth] = {};  // logical history slot -> physical buffer
     int cur = 0;               // physical buffer of the current iteration
     double DD[kRedWidth][kRedWidth] = {};

@@ -31,7 +31,7 @@ struct EnsRep {
     const cpx<float> *tw[3];
     const float *g[3];
     double *qpart, *Qd, *partials;
-    double *Dh[kRedWidth], *wh[kRedWidth];
+    float *Dh[kRedWidth], *wh[kRedWidth];  // FP32 history (the FP32-mixed context's)
     // Anderson loop state
     int phys[kRedWidth];  // logical history slot -> physical buffer
     int cur;              // physical buffer of the current iteration
@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(256) ens_update_kernel(EnsRep *__restrict__ re
         Dhp.p[m - 1] = R.Dh[R.phys[m]];
         whp.p[m - 1] = R.wh[R.phys[m]];
     }
-    anderson_update_body(R.w + R.M, R.wh[R.cur], R.Dh[R.cur], R.M, lambda[R.k], nh, R.simple, Dhp, whp, R.coef,
+    anderson_update_body<float>(R.w + R.M, R.wh[R.cur], R.Dh[R.cur], R.M, lambda[R.k], nh, R.simple, Dhp, whp, R.coef,
                          blockIdx.x, R.red_blocks);
 }
 

@@ -16,8 +16,11 @@ constexpr int kMaxHist = 10;          // anderson(M_, 10) (src/lfts_simulation.c
 constexpr int kRedWidth = kMaxHist + 1;
 constexpr int kRedThreads = 256;
 
+// Anderson history buffers; their element type is the context's propagator
+// type (FP64, or FP32 in the FP32-mixed path, where only the least squares,
+// Q and H are kept in FP64)
 struct HistPtrs {
-    const double *p[kMaxHist];
+    const void *p[kMaxHist];
 };
 struct Coefs {
     double c[kMaxHist];
@@ -77,10 +80,11 @@ template <typename T>
 __device__ __forceinline__ void concentrations_body(
     const T *__restrict__ q, long long M, int N, int NA, const double *__restrict__ w,
     double *__restrict__ phim, double *__restrict__ phip, const double *__restrict__ Qd,
-    double *__restrict__ Dh0, int nh, const HistPtrs &hist, double *__restrict__ partials, const int blk,
+    T *__restrict__ Dh0, int nh, const HistPtrs &hist, double *__restrict__ partials, const int blk,
     const int nblk)
 {
     constexpr int V = sizeof(T) == 4 ? 4 : 2;
+    using VT = typename VecOf<T, V>::type;
     __shared__ double sh[kRedThreads / 32];
     const double Q = Qd[0];
     const double NQ = __dmul_rn((double)N, Q);
@@ -131,17 +135,20 @@ __device__ __forceinline__ void concentrations_body(
                 d[j] = __dsub_rn(pp[j], 1.0);
                 acc[0] = __dadd_rn(acc[0], __dmul_rn(d[j], d[j]));
             }
+            {
+                VT dv;
+                T *e = reinterpret_cast<T *>(&dv);
 #pragma unroll
-            for (int j = 0; j < V; j += 2) *reinterpret_cast<double2 *>(Dh0 + r0 + j) = make_double2(d[j], d[j + 1]);
+                for (int j = 0; j < V; j++) e[j] = (T)d[j];
+                *reinterpret_cast<VT *>(Dh0 + r0) = dv;
+            }
 #pragma unroll
             for (int m = 1; m < kRedWidth; m++) {
                 if (m <= nh) {
+                    T hv[V];
+                    vload<T, V>(static_cast<const T *>(hist.p[m - 1]) + r0, hv);
 #pragma unroll
-                    for (int j = 0; j < V; j += 2) {
-                        const double2 hv = *reinterpret_cast<const double2 *>(hist.p[m - 1] + r0 + j);
-                        acc[m] = __dadd_rn(acc[m], __dmul_rn(d[j], hv.x));
-                        acc[m] = __dadd_rn(acc[m], __dmul_rn(d[j + 1], hv.y));
-                    }
+                    for (int j = 0; j < V; j++) acc[m] = __dadd_rn(acc[m], __dmul_rn(d[j], (double)hv[j]));
                 }
             }
         }
@@ -160,7 +167,7 @@ template <typename T>
 static __global__ void __launch_bounds__(kRedThreads, 4) concentrations_kernel(
     const T *__restrict__ q, long long M, int N, int NA, const double *__restrict__ w,
     double *__restrict__ phim, double *__restrict__ phip, const double *__restrict__ Qd,
-    double *__restrict__ Dh0, int nh, HistPtrs hist, double *__restrict__ partials)
+    T *__restrict__ Dh0, int nh, HistPtrs hist, double *__restrict__ partials)
 {
     concentrations_body<T>(q, M, N, NA, w, phim, phip, Qd, Dh0, nh, hist, partials, blockIdx.x, gridDim.x);
 }
@@ -179,23 +186,26 @@ static __global__ void reduce_partials_kernel(const double *partials, int nblock
 
 // w+ update of one Anderson iteration (src/anderson.cc:57-79) and the copy
 // of the pre-update w+ into the current history slot (wh_[0], :38).
-__device__ __forceinline__ void anderson_update_body(double *__restrict__ wp, double *__restrict__ wh0,
-                                                     const double *__restrict__ Dh0, long long M, double lambda,
+template <typename H>
+__device__ __forceinline__ void anderson_update_body(double *__restrict__ wp, H *__restrict__ wh0,
+                                                     const H *__restrict__ Dh0, long long M, double lambda,
                                                      int nh, int simple, const HistPtrs &Dh, const HistPtrs &wh,
                                                      const double *c, const int blk, const int nblk)
 {
     const long long stride = (long long)nblk * blockDim.x;
     for (long long r = (long long)blk * blockDim.x + threadIdx.x; r < M; r += stride) {
         const double old = wp[r];
-        const double d0 = Dh0[r];
-        wh0[r] = old;
+        const double d0 = (double)Dh0[r];
+        wh0[r] = (H)old;
         const double base = __dadd_rn(old, __dmul_rn(lambda, d0));
         double acc = base;
         if (!simple) {
 #pragma unroll
             for (int n = 0; n < kMaxHist; n++) {
                 if (n < nh) {
-                    const double hn = __dadd_rn(wh.p[n][r], __dmul_rn(lambda, Dh.p[n][r]));
+                    const double whn = (double)static_cast<const H *>(wh.p[n])[r];
+                    const double dhn = (double)static_cast<const H *>(Dh.p[n])[r];
+                    const double hn = __dadd_rn(whn, __dmul_rn(lambda, dhn));
                     acc = __dadd_rn(acc, __dmul_rn(c[n], __dsub_rn(hn, base)));
                 }
             }
@@ -204,11 +214,12 @@ __device__ __forceinline__ void anderson_update_body(double *__restrict__ wp, do
     }
 }
 
-static __global__ void anderson_update_kernel(double *__restrict__ wp, double *__restrict__ wh0,
-                                       const double *__restrict__ Dh0, long long M, double lambda,
-                                       int nh, int simple, HistPtrs Dh, HistPtrs wh, Coefs C)
+template <typename H>
+static __global__ void anderson_update_kernel(double *__restrict__ wp, H *__restrict__ wh0,
+                                              const H *__restrict__ Dh0, long long M, double lambda, int nh,
+                                              int simple, HistPtrs Dh, HistPtrs wh, Coefs C)
 {
-    anderson_update_body(wp, wh0, Dh0, M, lambda, nh, simple, Dh, wh, C.c, blockIdx.x, gridDim.x);
+    anderson_update_body<H>(wp, wh0, Dh0, M, lambda, nh, simple, Dh, wh, C.c, blockIdx.x, gridDim.x);
 }
 
 // W- += -(phi- + 2 W-/XbN) dt + (eta_prev + eta_new)/2   (src/langevin.cc:31)

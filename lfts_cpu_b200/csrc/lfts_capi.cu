@@ -335,12 +335,12 @@ void enqueue_chain_launches(lfts_ctx *c)
 }
 
 template <typename T>
-void enqueue_concs(lfts_ctx *c, double *Dh0, int nh, const HistPtrs &hist)
+void enqueue_concs(lfts_ctx *c, void *Dh0, int nh, const HistPtrs &hist)
 {
     enqueue_chain<T>(c);
     concentrations_kernel<T><<<stream_grid(c), kRedThreads, 0, c->st>>>(
         static_cast<const T *>(c->q), c->M, c->N, c->NA, c->w, c->w + 2 * c->M, c->w + 3 * c->M, c->Qd,
-        Dh0, nh, hist, c->partials);
+        static_cast<T *>(Dh0), nh, hist, c->partials);
     c->launches++;
     if (Dh0) {
         reduce_partials_kernel<<<1, 256, 0, c->st>>>(c->partials, c->red_blocks, nh + 1, c->red);
@@ -348,7 +348,7 @@ void enqueue_concs(lfts_ctx *c, double *Dh0, int nh, const HistPtrs &hist)
     }
 }
 
-void enqueue_concs_any(lfts_ctx *c, double *Dh0, int nh, const HistPtrs &hist)
+void enqueue_concs_any(lfts_ctx *c, void *Dh0, int nh, const HistPtrs &hist)
 {
     if (c->prec == LFTS_FP64)
         enqueue_concs<double>(c, Dh0, nh, hist);
@@ -517,7 +517,7 @@ int anderson_mix(lfts_ctx *c, int maxIter, double errTol, int *k_out)
             Dhp.p[m - 1] = c->Dh[c->phys[m]];
             whp.p[m - 1] = c->wh[c->phys[m]];
         }
-        double *Dh0 = c->Dh[c->cur];
+        void *Dh0 = c->Dh[c->cur];
         enqueue_concs_any(c, Dh0, nh, Dhp);
         CK(cudaMemcpyAsync(c->red_host, c->red, (nh + 1) * sizeof(double), cudaMemcpyDeviceToHost, c->st));
         CK(cudaStreamSynchronize(c->st));
@@ -544,8 +544,14 @@ int anderson_mix(lfts_ctx *c, int maxIter, double errTol, int *k_out)
                 return LFTS_ERR_SINGULAR;
             }
         }
-        anderson_update_kernel<<<stream_grid(c), 256, 0, c->st>>>(c->w + M, c->wh[c->cur], Dh0, M, lambda, nh,
-                                                                  simple, Dhp, whp, C);
+        if (c->prec == LFTS_FP64)
+            anderson_update_kernel<double><<<stream_grid(c), 256, 0, c->st>>>(
+                c->w + M, static_cast<double *>(c->wh[c->cur]), static_cast<const double *>(Dh0), M, lambda, nh,
+                simple, Dhp, whp, C);
+        else
+            anderson_update_kernel<float><<<stream_grid(c), 256, 0, c->st>>>(
+                c->w + M, static_cast<float *>(c->wh[c->cur]), static_cast<const float *>(Dh0), M, lambda, nh,
+                simple, Dhp, whp, C);
         c->launches++;
         CK(cudaGetLastError());
 
@@ -657,10 +663,10 @@ int ctx_alloc(lfts_ctx *c)
         CK(cudaMemset(c->eta[i], 0, sizeof(double) * M));
     }
     for (int i = 0; i < kRedWidth; i++) {
-        CK(cudaMalloc(&c->Dh[i], sizeof(double) * M));
-        CK(cudaMalloc(&c->wh[i], sizeof(double) * M));
-        CK(cudaMemset(c->Dh[i], 0, sizeof(double) * M));
-        CK(cudaMemset(c->wh[i], 0, sizeof(double) * M));
+        CK(cudaMalloc(&c->Dh[i], c->tsize * M));
+        CK(cudaMalloc(&c->wh[i], c->tsize * M));
+        CK(cudaMemset(c->Dh[i], 0, c->tsize * M));
+        CK(cudaMemset(c->wh[i], 0, c->tsize * M));
     }
     // logical slots 1..10 -> buffers 1..10, buffer 0 is the first current one
     for (int i = 0; i < kRedWidth; i++) c->phys[i] = i;
@@ -974,7 +980,7 @@ int lfts_device_bytes(const lfts_ctx *c, size_t *bytes)
     if (!c || !bytes) return LFTS_ERR_ARG;
     const size_t M = c->M;
     size_t b = 4 * M * 8 + c->tsize * 2 * M * c->N + c->tsize * 4 * (size_t)c->mx * c->my * c->KZ;
-    b += 2 * M * 8 + 2 * kRedWidth * M * 8 + c->Mk * 8;
+    b += 2 * M * 8 + 2 * kRedWidth * M * c->tsize + c->Mk * 8;
     if (c->sk_own_spec) b += c->Mk * 16;
     *bytes = b;
     return LFTS_OK;

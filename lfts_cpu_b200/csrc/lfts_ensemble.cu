@@ -365,8 +365,8 @@ int lfts_ensemble_create(const lfts_params *params, const unsigned long long *se
         R.Qd = c->Qd;
         R.partials = c->partials;
         for (int i = 0; i < kRedWidth; i++) {
-            R.Dh[i] = c->Dh[i];
-            R.wh[i] = c->wh[i];
+            R.Dh[i] = static_cast<float *>(c->Dh[i]);
+            R.wh[i] = static_cast<float *>(c->wh[i]);
             R.phys[i] = c->phys[i];
         }
         R.cur = c->cur;
