@@ -10,6 +10,10 @@
 // row-pair packing/unpacking and the packed Nyquist column, at the same FFT
 // count.  A 128x128 complex FP32 plane (139 KB with padding) fits one CTA.
 //
+// Stored propagators (FP32 packed path): slot i holds the M pairs
+// (q_i(r), q^_{N+1-i}(r)), one 8-byte store per mesh point; slot 1 is
+// (hA(r), hB(r)).
+//
 // Spectrum layout: full complex [x][ky][kz], kz in [0, mz); the x-pencil
 // kernel runs on it unchanged with ncol = my*mz and an even kz weight table.
 // Each CTA owns one x-plane; warps own whole z lines (rows) in the z section.
@@ -184,13 +188,34 @@ __device__ __forceinline__ void pc_z_fwdB(cpx<T> *P)
 
 // h values of this warp's stage-B tasks (rows in transposed y order); loaded
 // before the first z phase so the DRAM latency overlaps its shared-memory work.
+// 8-byte pair load / streaming store of the stored propagators
+__device__ __forceinline__ cpx<float> ld_pair(const cpx<float> *p)
+{
+    const float2 v = __ldg(reinterpret_cast<const float2 *>(p));
+    return {v.x, v.y};
+}
+__device__ __forceinline__ void st_pair(cpx<float> *p, float a, float b)
+{
+    __stcs(reinterpret_cast<float2 *>(p), make_float2(a, b));
+}
+__device__ __forceinline__ cpx<double> ld_pair(const cpx<double> *p)
+{
+    const double2 v = __ldg(reinterpret_cast<const double2 *>(p));
+    return {v.x, v.y};
+}
+__device__ __forceinline__ void st_pair(cpx<double> *p, double a, double b)
+{
+    __stcs(reinterpret_cast<double2 *>(p), make_double2(a, b));
+}
+
 template <typename C, typename T>
 struct PcH {
     static constexpr int R1 = C::RZ1, R2 = C::RZ2, NZ = R1 * R2;
     static constexpr int RND = (C::ROWS_PER_WARP * R1 + 31) / 32;
     T v[RND][R2][2];
-    // rounds [s0, s1) of this lane's tasks
-    __device__ __forceinline__ void load(const T *__restrict__ h1, const T *__restrict__ h2, int s0, int s1)
+    // rounds [s0, s1) of this lane's tasks; hp = this plane's (hA, hB) pairs,
+    // chain c takes hB when hsel_c = 1
+    __device__ __forceinline__ void load(const cpx<T> *__restrict__ hp, int hsel0, int hsel1, int s0, int s1)
     {
         int r0, nr;
         warp_rows<C>(threadIdx.x >> 5, r0, nr);
@@ -203,8 +228,9 @@ struct PcH {
                 const int y = C::ymap(r0 + t / R1), k1 = t % R1;
 #pragma unroll
                 for (int k2 = 0; k2 < R2; k2++) {
-                    v[s][k2][0] = __ldg(h1 + y * NZ + k1 + R1 * k2);
-                    v[s][k2][1] = __ldg(h2 + y * NZ + k1 + R1 * k2);
+                    const cpx<T> h = ld_pair(hp + y * NZ + k1 + R1 * k2);
+                    v[s][k2][0] = hsel0 ? h.y : h.x;
+                    v[s][k2][1] = hsel1 ? h.y : h.x;
                 }
             }
         }
@@ -215,7 +241,7 @@ struct PcH {
 // both propagators; STEP: forward stage B with twiddles; LAST: chain-1 sum.
 template <typename C, int MODE, typename T>
 __device__ __forceinline__ void pc_z_invB_h(cpx<T> *P, const cpx<T> *twb, const PcH<C, T> &hv,
-                                            T *__restrict__ q1, T *__restrict__ q2, double &qsum)
+                                            cpx<T> *__restrict__ qp, double &qsum)
 {
     constexpr int KP = C::KP, R1 = C::RZ1, R2 = C::RZ2, NZ = R1 * R2;
     constexpr int RND = PcH<C, T>::RND;
@@ -238,8 +264,7 @@ __device__ __forceinline__ void pc_z_invB_h(cpx<T> *P, const cpx<T> *twb, const 
             const int z = k1 + R1 * k2;
             const T a = v[k2].x * hv.v[s][k2][0];
             const T b = v[k2].y * hv.v[s][k2][1];
-            __stcs(q1 + y * NZ + z, a);
-            __stcs(q2 + y * NZ + z, b);
+            st_pair(qp + y * NZ + z, a, b);
             if (MODE == PLANE_LAST) qsum += (double)a;
             v[k2] = {a, b};
         }
@@ -328,8 +353,7 @@ __device__ __forceinline__ void plane_c_body(const PlaneArgs<T> &a, const int x,
                 const double wm = a.w[i], wp = a.w[M + i];
                 v1 = (T)exp(-(wm + wp) / a.Nd);
                 v2 = (T)exp(-(-wm + wp) / a.Nd);
-                a.qout[i] = v1;
-                a.qout[M + i] = v2;
+                reinterpret_cast<cpx<T> *>(a.qout)[i] = {v1, v2};
             } else if (a.src) {
                 v1 = a.src[i];
                 v2 = a.src[a.src_stride + i];
@@ -367,16 +391,14 @@ __device__ __forceinline__ void plane_c_body(const PlaneArgs<T> &a, const int x,
     // h of the first stage-B round goes out before the first z phase, the
     // rest after it (register budget)
     PcH<C, T> hv;
-    const T *h1 = a.h + (long long)a.hsel0 * M + plane_off;
-    const T *h2 = a.h + (long long)a.hsel1 * M + plane_off;
-    hv.load(h1, h2, 0, 1);
+    const cpx<T> *hp = reinterpret_cast<const cpx<T> *>(a.h) + plane_off;
+    hv.load(hp, a.hsel0, a.hsel1, 0, 1);
     pc_z_A<C, 1, true>(P, twa);
-    hv.load(h1, h2, 1, PcH<C, T>::RND);
+    hv.load(hp, a.hsel0, a.hsel1, 1, PcH<C, T>::RND);
     __syncwarp();
-    T *q1 = a.qout + plane_off;
-    T *q2 = a.qout + M + plane_off;
+    cpx<T> *qp = reinterpret_cast<cpx<T> *>(a.qout) + plane_off;
     double qsum = 0.0;
-    pc_z_invB_h<C, MODE>(P, twb, hv, q1, q2, qsum);
+    pc_z_invB_h<C, MODE>(P, twb, hv, qp, qsum);
     if (MODE == PLANE_LAST) {
         __shared__ double red[C::NT / 32];
         for (int o = 16; o > 0; o >>= 1) qsum += __shfl_xor_sync(0xffffffffu, qsum, o);

@@ -23,7 +23,7 @@
 // jz + 16 c1 (S2, S3), so every stage is in place.  Row pitch 136 = 8 (mod 16)
 // slots: the half-warps of each access pattern hit distinct bank pairs.
 #pragma once
-#include "fft_kernels.cuh"
+#include "fft_packed.cuh"
 
 namespace lfts {
 
@@ -154,10 +154,10 @@ __device__ __forceinline__ void p3_s3(cpx<float> *P, const PlaneArgs<float> &a, 
                                       double &qsum)
 {
     using C = Plane3Cfg;
-    const float *__restrict__ h1 = a.h + (long long)a.hsel0 * M + plane_off;
-    const float *__restrict__ h2 = a.h + (long long)a.hsel1 * M + plane_off;
-    float *__restrict__ q1 = a.qout + plane_off;
-    float *__restrict__ q2 = a.qout + M + plane_off;
+    // stored propagators and h as (chain 1, chain 2) pairs (fft_packed.cuh)
+    const cpx<float> *__restrict__ hp = reinterpret_cast<const cpx<float> *>(a.h) + plane_off;
+    cpx<float> *__restrict__ qp = reinterpret_cast<cpx<float> *>(a.qout) + plane_off;
+    const int hs0 = a.hsel0, hs1 = a.hsel1;
 #pragma unroll 1
     for (int s = 0; s < 2; s++) {
         const int u = threadIdx.x + 512 * s;
@@ -166,8 +166,9 @@ __device__ __forceinline__ void p3_s3(cpx<float> *P, const PlaneArgs<float> &a, 
         float ha[16], hb[16];
 #pragma unroll
         for (int c2 = 0; c2 < 16; c2++) {
-            ha[c2] = __ldg(h1 + y * 128 + c1 + 8 * c2);
-            hb[c2] = __ldg(h2 + y * 128 + c1 + 8 * c2);
+            const cpx<float> h = ld_pair(hp + y * 128 + c1 + 8 * c2);
+            ha[c2] = hs0 ? h.y : h.x;
+            hb[c2] = hs1 ? h.y : h.x;
         }
         cpx<float> g[16];
 #pragma unroll
@@ -178,8 +179,7 @@ __device__ __forceinline__ void p3_s3(cpx<float> *P, const PlaneArgs<float> &a, 
             const int z = c1 + 8 * c2;
             const float va = g[c2].x * ha[c2];
             const float vb = g[c2].y * hb[c2];
-            __stcs(q1 + y * 128 + z, va);
-            __stcs(q2 + y * 128 + z, vb);
+            st_pair(qp + y * 128 + z, va, vb);
             if (MODE == PLANE_LAST) qsum += (double)va;
             g[c2] = {va, vb};
         }
@@ -211,8 +211,7 @@ __device__ __forceinline__ void p3_s3_init(cpx<float> *P, const PlaneArgs<float>
                 const double wm = a.w[i], wp = a.w[M + i];
                 v1 = expf((float)(-(wm + wp) / a.Nd));
                 v2 = expf((float)(-(-wm + wp) / a.Nd));
-                a.qout[i] = v1;
-                a.qout[M + i] = v2;
+                reinterpret_cast<cpx<float> *>(a.qout)[i] = {v1, v2};
             } else if (a.src) {
                 v1 = a.src[i];
                 v2 = a.src[a.src_stride + i];

@@ -99,22 +99,59 @@ __device__ __forceinline__ void concentrations_body(
         double sA[V], sB[V];
 #pragma unroll
         for (int j = 0; j < V; j++) sA[j] = sB[j] = 0.0;
-#pragma unroll 8
-        for (int i = 1; i <= N; i++) {
-            T a[V], b[V];
-            vload<T, V>(q + (long long)(i - 1) * 2 * M + r0, a);
-            vload<T, V>(q + (long long)(N - i) * 2 * M + M + r0, b);
-            if (i <= NA) {
-#pragma unroll
-                for (int j = 0; j < V; j++) sA[j] = __dadd_rn(sA[j], __dmul_rn((double)a[j], (double)b[j]));
-            } else {
-#pragma unroll
-                for (int j = 0; j < V; j++) sB[j] = __dadd_rn(sB[j], __dmul_rn((double)a[j], (double)b[j]));
-            }
-        }
         T hA[V], hB[V];
-        vload<T, V>(q + r0, hA);
-        vload<T, V>(q + M + r0, hB);
+        if constexpr (sizeof(T) == 4) {
+            // FP32 packed layout: slot i holds pairs (q_i, q^_{N+1-i}) (fft_packed.cuh),
+            // so slots i and j = N+1-i together give q_i q^_i and q_j q^_j
+#pragma unroll 4
+            for (int i = 1; 2 * i <= N + 1; i++) {
+                const int j = N + 1 - i;
+                T a[2 * V], b[2 * V];
+                vload<T, V>(q + (long long)(i - 1) * 2 * M + 2 * r0, *reinterpret_cast<T(*)[V]>(a));
+                vload<T, V>(q + (long long)(i - 1) * 2 * M + 2 * r0 + V, *reinterpret_cast<T(*)[V]>(a + V));
+                vload<T, V>(q + (long long)(j - 1) * 2 * M + 2 * r0, *reinterpret_cast<T(*)[V]>(b));
+                vload<T, V>(q + (long long)(j - 1) * 2 * M + 2 * r0 + V, *reinterpret_cast<T(*)[V]>(b + V));
+#pragma unroll
+                for (int p = 0; p < V; p++) {
+                    const double pi = __dmul_rn((double)a[2 * p], (double)b[2 * p + 1]);  // q_i q^_i
+                    if (i <= NA)
+                        sA[p] = __dadd_rn(sA[p], pi);
+                    else
+                        sB[p] = __dadd_rn(sB[p], pi);
+                    if (j != i) {
+                        const double pj = __dmul_rn((double)b[2 * p], (double)a[2 * p + 1]);  // q_j q^_j
+                        if (j <= NA)
+                            sA[p] = __dadd_rn(sA[p], pj);
+                        else
+                            sB[p] = __dadd_rn(sB[p], pj);
+                    }
+                }
+            }
+            T h[2 * V];
+            vload<T, V>(q + 2 * r0, *reinterpret_cast<T(*)[V]>(h));
+            vload<T, V>(q + 2 * r0 + V, *reinterpret_cast<T(*)[V]>(h + V));
+#pragma unroll
+            for (int p = 0; p < V; p++) {
+                hA[p] = h[2 * p];
+                hB[p] = h[2 * p + 1];
+            }
+        } else {
+#pragma unroll 8
+            for (int i = 1; i <= N; i++) {
+                T a[V], b[V];
+                vload<T, V>(q + (long long)(i - 1) * 2 * M + r0, a);
+                vload<T, V>(q + (long long)(N - i) * 2 * M + M + r0, b);
+                if (i <= NA) {
+#pragma unroll
+                    for (int j = 0; j < V; j++) sA[j] = __dadd_rn(sA[j], __dmul_rn((double)a[j], (double)b[j]));
+                } else {
+#pragma unroll
+                    for (int j = 0; j < V; j++) sB[j] = __dadd_rn(sB[j], __dmul_rn((double)a[j], (double)b[j]));
+                }
+            }
+            vload<T, V>(q + r0, hA);
+            vload<T, V>(q + M + r0, hB);
+        }
         double pm[V], pp[V];
 #pragma unroll
         for (int j = 0; j < V; j++) {
@@ -270,6 +307,27 @@ static __global__ void sk_bin_kernel(const double *__restrict__ S, const int *__
         n += wt[p];
     }
     out[b] = s / (double)n;
+}
+
+// [a | b] halves (M each) <-> M pairs (a, b): the FP32 packed path stores h
+// and the propagators as pairs
+template <typename Tin, typename Tout>
+static __global__ void to_pairs_kernel(const Tin *__restrict__ in, Tout *__restrict__ out, long long M)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < M; r += stride) {
+        out[2 * r] = (Tout)in[r];
+        out[2 * r + 1] = (Tout)in[M + r];
+    }
+}
+template <typename Tin, typename Tout>
+static __global__ void from_pairs_kernel(const Tin *__restrict__ in, Tout *__restrict__ out, long long M)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < M; r += stride) {
+        out[r] = (Tout)in[2 * r];
+        out[M + r] = (Tout)in[2 * r + 1];
+    }
 }
 
 template <typename Tin, typename Tout>

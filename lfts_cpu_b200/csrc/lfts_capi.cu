@@ -750,7 +750,7 @@ int step_fwd_impl(lfts_ctx *c, const double *q_in, double *q_out, const double *
     T *dst = reinterpret_cast<T *>(dout);
     if (sizeof(T) != sizeof(double)) {
         convert_kernel<double, T><<<stream_grid(c), 256, 0, c->st>>>(dq, tq, 2 * M);
-        convert_kernel<double, T><<<stream_grid(c), 256, 0, c->st>>>(dh, th, 2 * M);
+        to_pairs_kernel<double, T><<<stream_grid(c), 256, 0, c->st>>>(dh, th, M);  // packed-path layout
         c->launches += 2;
         src = tq;
         hh = th;
@@ -767,7 +767,7 @@ int step_fwd_impl(lfts_ctx *c, const double *q_in, double *q_out, const double *
     a.hsel1 = hsel_chain1(c, i);
     launch_plane<T>(c, PLANE_LAST, a, 2);
     if (sizeof(T) != sizeof(double)) {
-        convert_kernel<T, double><<<stream_grid(c), 256, 0, c->st>>>(tout, dout, 2 * M);
+        from_pairs_kernel<T, double><<<stream_grid(c), 256, 0, c->st>>>(tout, dout, M);
         c->launches++;
     }
     CK(cudaGetLastError());
@@ -1305,10 +1305,19 @@ int lfts_get_propagators(lfts_ctx *c, double *q_host)
         CK(cudaMemcpyAsync(q_host + 2 * c->M, c->q, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
         CK(cudaStreamSynchronize(c->st));
     } else {
+        // FP32 slots hold (q_i, q^_{N+1-i}) pairs: back to the [q_i | q^] halves
         std::vector<float> tmp(n);
         CK(cudaMemcpyAsync(tmp.data(), c->q, sizeof(float) * n, cudaMemcpyDeviceToHost, c->st));
         CK(cudaStreamSynchronize(c->st));
-        for (long long i = 0; i < n; i++) q_host[2 * c->M + i] = tmp[i];
+        const long long M = c->M;
+        for (int sl = 0; sl < c->N; sl++) {
+            const float *src = tmp.data() + (long long)sl * 2 * M;
+            double *dst = q_host + (long long)(sl + 1) * 2 * M;
+            for (long long r = 0; r < M; r++) {
+                dst[r] = src[2 * r];
+                dst[M + r] = src[2 * r + 1];
+            }
+        }
     }
     return LFTS_OK;
 }

@@ -200,3 +200,23 @@ def test_full_size_identities_128(lfts, precision):
         s64.set_fields(w2)
         s64.calc_concs()
         assert rel_err(w[2 * M:], s64.get_fields()[2 * M:]) < FP32_PHI_TOL
+
+
+@pytest.mark.parametrize("name", ["comp_16", "comp_12x24x16"])
+def test_fp32_step_and_propagators_layout(lfts, name):
+    """The FP32 path stores (q_i, q^_{N+1-i}) pairs internally; step_fwd and
+    get_propagators return the reference's [q_i | q^] halves, equal to the
+    FP64 results within the FP32 tolerance."""
+    g = golden(name)
+    s64, M = make_system(lfts, g)
+    s32, _ = make_system(lfts, g, precision=lfts.LFTS_FP32_MIXED)
+    for i in g["steps"]:
+        a = s64.step_fwd(g["q_in"], g["h"], int(i))
+        b = s32.step_fwd(g["q_in"], g["h"], int(i))
+        assert rel_err(b, a) < 1e-5
+    for s in (s64, s32):
+        s.set_fields(g["w_in"])
+        s.calc_concs()
+    p64, p32 = s64.propagators().ravel(), s32.propagators().ravel()
+    assert np.all(p32[: 2 * M] == 0.0)
+    assert rel_err(p32, p64) < 1e-5
