@@ -19,9 +19,11 @@
 //             S1  DFT-32 over k1                                       smem -> global
 //
 // Shared-memory rows hold (after S1) T[j2][k1] at row k1 + 32 j2, and (after
-// S2) natural y; columns are at pos(p) = p + p/16 with p = kz (S1) or
-// jz + 16 c1 (S2, S3), so every stage is in place.  Row pitch 136 = 8 (mod 16)
-// slots: the half-warps of each access pattern hit distinct bank pairs.
+// S2) natural y; columns are at pos(p) = p + 2 (p/16) with p = kz (S1) or
+// jz + 16 c1 (S2, S3), so every stage is in place.  The two pad slots per 16
+// make each S3 task's 16 values one 16-byte-aligned run (read and written with
+// 16-byte accesses, conflict-free per quarter-warp); the S1/S2 half-warps read
+// 16 consecutive slots of one row.  Row pitch 142 slots.
 #pragma once
 #include "fft_packed.cuh"
 
@@ -30,12 +32,29 @@ namespace lfts {
 struct Plane3Cfg {
     static constexpr int N = 128;
     static constexpr int NT = 512;
-    static constexpr int KP = 136;
+    static constexpr int KP = 142;
     // TY[j2 * 32 + k1] = w^(j2 k1), TZ[c1 * 16 + jz] = w^(jz c1), w = exp(-2 pi i/128)
     static constexpr size_t TOFF = sizeof(cpx<float>) * (size_t)(N * KP);
     static constexpr size_t SMEM = TOFF + sizeof(cpx<float>) * 256;
-    static __device__ __forceinline__ int pos(int p) { return p + (p >> 4); }
+    static __device__ __forceinline__ int pos(int p) { return p + 2 * (p >> 4); }
 };
+
+// the 16 values of an S3 task: row[pos(16 c1) .. +15], 16-byte aligned
+__device__ __forceinline__ void p3_ld16(const cpx<float> *run, cpx<float> (&g)[16])
+{
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+        const float4 v = reinterpret_cast<const float4 *>(run)[m];
+        g[2 * m] = {v.x, v.y};
+        g[2 * m + 1] = {v.z, v.w};
+    }
+}
+__device__ __forceinline__ void p3_st16(cpx<float> *run, const cpx<float> (&g)[16])
+{
+#pragma unroll
+    for (int m = 0; m < 8; m++)
+        reinterpret_cast<float4 *>(run)[m] = make_float4(g[2 * m].x, g[2 * m].y, g[2 * m + 1].x, g[2 * m + 1].y);
+}
 
 // S1 inverse: one (kz, j2) task per thread, 32 strided rows from the global spectrum
 __device__ __forceinline__ void p3_s1_inv(cpx<float> *P, const cpx<float> *__restrict__ Sg)
@@ -171,8 +190,7 @@ __device__ __forceinline__ void p3_s3(cpx<float> *P, const PlaneArgs<float> &a, 
             hb[c2] = hs1 ? h.y : h.x;
         }
         cpx<float> g[16];
-#pragma unroll
-        for (int jz = 0; jz < 16; jz++) g[jz] = row[C::pos(jz + 16 * c1)];
+        p3_ld16(row + C::pos(16 * c1), g);
         Dft<16, 1, float>::run(g);
 #pragma unroll
         for (int c2 = 0; c2 < 16; c2++) {
@@ -185,8 +203,7 @@ __device__ __forceinline__ void p3_s3(cpx<float> *P, const PlaneArgs<float> &a, 
         }
         if (MODE == PLANE_STEP) {
             Dft<16, -1, float>::run(g);
-#pragma unroll
-            for (int jz = 0; jz < 16; jz++) row[C::pos(jz + 16 * c1)] = g[jz];
+            p3_st16(row + C::pos(16 * c1), g);
         }
     }
 }
@@ -222,9 +239,7 @@ __device__ __forceinline__ void p3_s3_init(cpx<float> *P, const PlaneArgs<float>
             g[c2] = {v1, v2};
         }
         Dft<16, -1, float>::run(g);
-        cpx<float> *row = P + y * C::KP;
-#pragma unroll
-        for (int jz = 0; jz < 16; jz++) row[C::pos(jz + 16 * c1)] = g[jz];
+        p3_st16(P + y * C::KP + C::pos(16 * c1), g);
     }
 }
 
