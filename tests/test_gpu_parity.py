@@ -220,3 +220,32 @@ def test_fp32_step_and_propagators_layout(lfts, name):
     p64, p32 = s64.propagators().ravel(), s32.propagators().ravel()
     assert np.all(p32[: 2 * M] == 0.0)
     assert rel_err(p32, p64) < 1e-5
+
+
+@pytest.mark.parametrize("NA,NB", [(0, 8), (8, 0), (1, 1), (3, 4), (4, 3)])
+def test_chain_edges_match_oracle(lfts, oracle_built, NA, NB):
+    """Pure-A / pure-B chains, N = 2 and odd N through the C ABI: FP64 equals
+    the oracle to 1e-10 (calc_concs, mix), FP32-mixed to its tolerance."""
+    from pyoracle import Oracle
+    m, L = (8, 12, 20), (2.0, 2.5, 3.0)
+    M = int(np.prod(m))
+    N = NA + NB
+    rng = np.random.default_rng(NA * 10 + NB)
+    w = np.zeros(4 * M)
+    w[:2 * M] = rng.normal(0.0, 0.8, 2 * M)
+    o = Oracle(NA, NB, m, L)
+    ref = w.copy()
+    lnq_ref = o.calc_concs(ref)
+    for prec, tol in ((0, FP64_TOL), (1, FP32_PHI_TOL)):
+        s = lfts.System(N, NA, 13.0, 50.0, 0.5, m, L, precision=prec)
+        s.set_fields(w[:2 * M])
+        lnq = s.calc_concs()
+        assert abs(lnq - lnq_ref) < tol * max(1.0, abs(lnq_ref))
+        assert rel_err(s.get_fields()[2 * M:], ref[2 * M:]) < tol
+        wm = w.copy()
+        k_ref = o.mix(wm)
+        if prec == 0 and np.all(np.isfinite(wm)):  # NB = 0: the reference's mix diverges to NaN
+            assert s.mix() == k_ref
+            assert rel_err(s.get_fields()[M:2 * M], wm[M:2 * M]) < 1e-9
+        s.close()
+    o.close()

@@ -168,3 +168,30 @@ def test_lamellar_mix_is_roundoff_sensitive(Oracle, native_lib):
     assert rel_err(out[0][1], g["w0"]) < 1e-12
     assert out[0][0] != out[1][0]
     assert rel_err(out[1][1], out[0][1]) > 1e-7
+
+
+EDGE_CHAINS = [(0, 8), (8, 0), (1, 1), (3, 4), (4, 3)]  # NA, NB: homopolymer ends, N = 2, odd N
+
+
+@pytest.mark.parametrize("NA,NB", EDGE_CHAINS)
+def test_oracle_matches_reference_chain_edges(oracle_built, NA, NB):
+    """Pure-A / pure-B chains, the shortest chain and odd N: the restatement
+    equals the reference's own classes (shim build) bitwise, calc_concs and mix."""
+    from pyoracle import Oracle, RefHarness, RefSys
+    if not RefHarness.available():
+        pytest.skip("oracle/_ref not built (needs the reference tree)")
+    m, L = (8, 12, 20), (2.0, 2.5, 3.0)
+    M = int(np.prod(m))
+    rng = np.random.default_rng(NA * 10 + NB)
+    w = np.zeros(4 * M)
+    w[:2 * M] = rng.normal(0.0, 0.8, 2 * M)
+    a, b = w.copy(), w.copy()
+    o, r = Oracle(NA, NB, m, L), RefSys(NA, NB, m, L)
+    assert o.calc_concs(a) == r.calc_concs(b)
+    assert np.array_equal(a, b)
+    a[2 * M:] = 0.0
+    b[2 * M:] = 0.0
+    assert o.mix(a) == r.mix(b)
+    assert np.array_equal(a, b, equal_nan=True)  # NB = 0: the reference's mix diverges to NaN
+    o.close()
+    r.close()
