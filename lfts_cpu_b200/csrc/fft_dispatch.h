@@ -29,7 +29,6 @@ bool plane_c_kernels(int ny, int nz, PlaneKernels<float> *out);
 // three-stage packed-chain plane kernels (fft_plane3.cuh), FP32, 128 x 128 only
 bool plane3_kernels(int ny, int nz, PlaneKernels<float> *out);
 bool plane_kernels(int ny, int nz, PlaneKernels<double> *out);
-bool plane_kernels(int ny, int nz, PlaneKernels<float> *out);
 bool pencil_kernels(int nx, PencilKernels<double> *out);
 bool pencil_kernels(int nx, PencilKernels<float> *out);
 // x-pencil kernels of tile width cw (columns per CTA: 8, 16 or 32); the tile

@@ -2,8 +2,6 @@
 #include "fft_inst.cuh"
 #include "fft_plane3.cuh"
 
-#define LFTS_PLANE_CASE_float(a, b) \
-    if (ny == a && nz == b) { fill_plane<float, a, b>(o); return true; }
 #define LFTS_PENCIL_CASE_float(a) \
     if (nx == a) { fill_pencil<float, a>(o); return true; }
 #define LFTS_PENCIL_CW_CASE_float(a)                                   \

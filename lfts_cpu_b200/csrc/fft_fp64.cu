@@ -12,6 +12,7 @@
         if (cw == 32) { fill_pencil<double, a, 32>(o); return true; }    \
         return false;                                                \
     }
+LFTS_DEFINE_PLANE_DISPATCH(double)
 LFTS_DEFINE_DISPATCH(double)
 
 namespace lfts {

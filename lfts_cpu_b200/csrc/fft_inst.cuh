@@ -41,7 +41,11 @@ static void fill_pencil(PencilKernels<T> *o)
 {
     using C = PencilCfg<T, NX, CW>;
     o->fn[PENCIL_CONV] = pencil_kernel<T, NX, CW, PENCIL_CONV>;
-    o->fn[PENCIL_POWER] = pencil_kernel<T, NX, CW, PENCIL_POWER>;
+    // S(k) samples run in FP64 in both precisions
+    if constexpr (sizeof(T) == sizeof(double))
+        o->fn[PENCIL_POWER] = pencil_kernel<T, NX, CW, PENCIL_POWER>;
+    else
+        o->fn[PENCIL_POWER] = nullptr;
     o->nt = C::NT;
     o->smem = C::SMEM;
     o->cw = CW;
@@ -49,13 +53,18 @@ static void fill_pencil(PencilKernels<T> *o)
 
 }  // namespace lfts
 
-#define LFTS_DEFINE_DISPATCH(T)                                                       \
+// pencils of one precision (both); half-spectrum plane kernels (FP64 only:
+// FP32 contexts use the packed-field kernels)
+#define LFTS_DEFINE_PLANE_DISPATCH(T)                                                 \
     namespace lfts {                                                                  \
     bool plane_kernels(int ny, int nz, PlaneKernels<T> *o)                            \
     {                                                                                 \
         LFTS_FOR_EACH_PAIR(LFTS_PLANE_CASE_##T)                                       \
         return false;                                                                 \
     }                                                                                 \
+    }
+#define LFTS_DEFINE_DISPATCH(T)                                                       \
+    namespace lfts {                                                                  \
     bool pencil_kernels(int nx, PencilKernels<T> *o)                                  \
     {                                                                                 \
         LFTS_FOR_EACH_LEN(LFTS_PENCIL_CASE_##T)                                       \

@@ -124,7 +124,7 @@ int set_smem_attrs(const PlaneKernels<T> &pl, const PencilKernels<T> &pe)
     for (int m = 0; m < 4; m++)
         CK(cudaFuncSetAttribute(pl.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
     for (int m = 0; m < 2; m++)
-        CK(cudaFuncSetAttribute(pe.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pe.smem));
+        if (pe.fn[m]) CK(cudaFuncSetAttribute(pe.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pe.smem));
     return LFTS_OK;
 }
 
@@ -370,7 +370,7 @@ int set_pencil(lfts_ctx *c, int cw)
     PencilKernels<T> pk{};
     if (!pencil_kernels(c->mx, cw, &pk)) return LFTS_ERR_UNSUPPORTED;
     for (int m = 0; m < 2; m++)
-        CK(cudaFuncSetAttribute(pk.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pk.smem));
+        if (pk.fn[m]) CK(cudaFuncSetAttribute(pk.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pk.smem));
     pencil_of<T>(c) = pk;
     return LFTS_OK;
 }

@@ -108,3 +108,20 @@ def test_batched_configuration_shape(lfts):
         assert lnq[r] == slnq
         assert np.array_equal(e.get_fields(r), sw)
     e.close()
+
+
+def test_ensemble_rejects_bad_input(lfts):
+    from lfts_cpu_b200.capi import LftsError
+    base = dict(N=12, NA=5, XbN=13.0, C=50.0, dt=0.5, m=(16, 16, 16), L=(3.0, 3.0, 3.0), seed=1)
+    with pytest.raises(LftsError) as e:
+        lfts.Ensemble([base, dict(base, m=(128, 128, 128), L=(8.0, 8.0, 8.0))])
+    assert e.value.status == 2  # unsupported mesh
+    with pytest.raises(LftsError) as e:
+        lfts.Ensemble([base, dict(base, N=14)])
+    assert e.value.status == 1  # replicas must share N
+    ens = lfts.Ensemble([base])
+    from lfts_cpu_b200.capi import lib
+    assert lib().lfts_ensemble_get_fields(ens._h, 1, np.empty(8)) == 1  # replica index out of range
+    with pytest.raises(LftsError):
+        ens.mix(max_iter=1)
+    ens.close()
