@@ -160,7 +160,7 @@ long long lfts_kernel_launches(const lfts_ctx *ctx);
  * (picked at lfts_create by timing the chain for 8, 16 and 32 columns, once
  * per precision and mesh in a process; LFTS_AUTOTUNE=0 in the environment
  * keeps the built-in width, LFTS_PENCIL_CW=8|16|32 forces one) and yz-plane
- * transform stages per axis (2; 3 for FP32-mixed 128 x 128 planes).  The tile
+ * transform stages per axis (2; 3 for FP32-mixed 64, 96, 128 square planes).  The tile
  * width does not change results. */
 int lfts_tuning(const lfts_ctx *ctx, int *pencil_cw, int *plane_stages);
 /* Mean Anderson iteration count of all lfts_anderson_mix calls so far. */

@@ -13,6 +13,7 @@
 // until every replica is done; the control kernel ends the WHILE loop then.
 #pragma once
 #include "fft_packed.cuh"
+#include "fft_plane3.cuh"
 #include "field_kernels.cuh"
 #include "philox.cuh"
 
@@ -67,6 +68,32 @@ __global__ void __launch_bounds__(PlaneCCfg<float, NY, NZ>::NT, 1)
         a.hsel1 = i < R.NB ? 1 : 0;               // src/step.cc:60-64
     }
     plane_c_body<float, NY, NZ, MODE>(a, blockIdx.x, R.mx);
+}
+
+// the three-stage plane body (64, 96, 128 planes), as the single context uses
+template <typename C3, int MODE>
+__global__ void __launch_bounds__(C3::NT, 1)
+    ens_plane3_kernel(EnsRep *__restrict__ reps, const int *__restrict__ members, int i)
+{
+    const EnsRep &R = reps[members[blockIdx.y]];
+    if (!R.active) return;
+    PlaneArgs<float> a{};
+    a.w = R.w;
+    a.spec = R.spec;
+    a.twy = R.tw[1];
+    a.twz = R.tw[2];
+    a.qpart = R.qpart;
+    a.nchains = 2;
+    a.Nd = (double)R.N;
+    if (MODE == PLANE_INIT_W) {
+        a.qout = R.q;
+    } else {
+        a.h = R.q;
+        a.qout = R.q + (long long)i * 2 * R.M;
+        a.hsel0 = i < R.NA ? 0 : 1;
+        a.hsel1 = i < R.NB ? 1 : 0;
+    }
+    plane3_body<C3, MODE>(a, blockIdx.x, R.mx);
 }
 
 template <int NX, int CW>

@@ -26,7 +26,7 @@ struct PencilKernels {
 // false when (ny, nz) / nx has no instantiation in this build
 // packed-chain plane kernels (fft_packed.cuh), FP32
 bool plane_c_kernels(int ny, int nz, PlaneKernels<float> *out);
-// three-stage packed-chain plane kernels (fft_plane3.cuh), FP32, 128 x 128 only
+// three-stage packed-chain plane kernels (fft_plane3.cuh), FP32: 64, 96, 128 square planes
 bool plane3_kernels(int ny, int nz, PlaneKernels<float> *out);
 bool plane_kernels(int ny, int nz, PlaneKernels<double> *out);
 bool pencil_kernels(int nx, PencilKernels<double> *out);

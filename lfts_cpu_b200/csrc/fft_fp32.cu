@@ -21,15 +21,22 @@ bool plane_c_kernels(int ny, int nz, PlaneKernels<float> *o)
     LFTS_FOR_EACH_PAIR(LFTS_PLANE_C_CASE)
     return false;
 }
+template <typename C>
+static void fill_plane3(PlaneKernels<float> *o)
+{
+    o->fn[PLANE_INIT_W] = plane3_kernel<C, PLANE_INIT_W>;
+    o->fn[PLANE_INIT_Q] = plane3_kernel<C, PLANE_INIT_Q>;
+    o->fn[PLANE_STEP] = plane3_kernel<C, PLANE_STEP>;
+    o->fn[PLANE_LAST] = plane3_kernel<C, PLANE_LAST>;
+    o->nt = C::NT;
+    o->smem = C::SMEM;
+}
 bool plane3_kernels(int ny, int nz, PlaneKernels<float> *o)
 {
-    if (ny != 128 || nz != 128) return false;
-    o->fn[PLANE_INIT_W] = plane3_kernel<PLANE_INIT_W>;
-    o->fn[PLANE_INIT_Q] = plane3_kernel<PLANE_INIT_Q>;
-    o->fn[PLANE_STEP] = plane3_kernel<PLANE_STEP>;
-    o->fn[PLANE_LAST] = plane3_kernel<PLANE_LAST>;
-    o->nt = Plane3Cfg::NT;
-    o->smem = Plane3Cfg::SMEM;
-    return true;
+    if (ny != nz) return false;
+    if (ny == 128) { fill_plane3<Plane3_128>(o); return true; }
+    if (ny == 96) { fill_plane3<Plane3_96>(o); return true; }
+    if (ny == 64) { fill_plane3<Plane3_64>(o); return true; }
+    return false;
 }
 }  // namespace lfts

@@ -75,9 +75,30 @@ void fill_pencil(PencilSet *o)
     o->smem = C::SMEM;
 }
 
+template <typename C3>
+void fill_plane3(PlaneSet *o)
+{
+    o->fn[PLANE_INIT_W] = ens_plane3_kernel<C3, PLANE_INIT_W>;
+    o->fn[PLANE_INIT_Q] = ens_plane3_kernel<C3, PLANE_INIT_Q>;
+    o->fn[PLANE_STEP] = ens_plane3_kernel<C3, PLANE_STEP>;
+    o->fn[PLANE_LAST] = ens_plane3_kernel<C3, PLANE_LAST>;
+    o->nt = C3::NT;
+    o->smem = C3::SMEM;
+}
+
+// the plane kernel a single FP32 context of this mesh uses (plane3_kernels /
+// plane_c_kernels), so that replicas reproduce single contexts
 bool ens_plane(int ny, int nz, PlaneSet *o)
 {
     if (ny != nz) return false;
+    if (ny == 96) {
+        fill_plane3<Plane3_96>(o);
+        return true;
+    }
+    if (ny == 64) {
+        fill_plane3<Plane3_64>(o);
+        return true;
+    }
 #define X(n)                    \
     if (ny == n) {              \
         fill_plane<n>(o);       \

@@ -46,7 +46,8 @@ def test_pencil_tile_width_is_bitwise_neutral(lfts, precision, m, N, NA):
 
 def test_autotuned_choices(lfts):
     os.environ.pop("LFTS_PENCIL_CW", None)
-    for precision, m, stages in ((1, (128, 128, 128), 3), (1, (64, 64, 64), 2), (0, (128, 128, 128), 2)):
+    for precision, m, stages in ((1, (128, 128, 128), 3), (1, (96, 96, 96), 3), (1, (64, 64, 64), 3),
+                                 (1, (48, 48, 48), 2), (0, (128, 128, 128), 2)):
         s = lfts.System(8, 3, 16.0, 100.0, 0.5, m, (4.0, 4.0, 4.0), precision=precision)
         cw, st = s.tuning()
         assert cw in (8, 16, 32)
