@@ -17,6 +17,7 @@ total steps of all ranks / max elapsed over ranks.
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import os
 import statistics
@@ -51,9 +52,10 @@ def measured_peak():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region
+    (every 50 ms, time-stamped; samples outside [begin, end] are dropped)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -61,16 +63,37 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.t_begin = self.t_end = None
 
     def start(self):
+        """Start sampling; returns once the first sample is written (at most 5 s)."""
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None and os.path.getsize(self.path) == 0:
+            time.sleep(0.02)
+
+    def begin(self):
+        self.t_begin = time.time()
+
+    def end(self):
+        self.t_end = time.time()
+
+    @staticmethod
+    def _stamp(text):
+        for fmt in ("%Y/%m/%d %H:%M:%S.%f", "%Y/%m/%d %H:%M:%S"):
+            try:
+                return datetime.datetime.strptime(text, fmt).timestamp()
+            except ValueError:
+                pass
+        return None
 
     def stop(self):
         out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
@@ -81,23 +104,28 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for line in open(self.path):
             f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sm.append(float(f[1]))
-                mx.append(float(f[2]))
+                rows.append((self._stamp(f[0]), float(f[2]), float(f[3]), f[6:10]))
             except ValueError:
                 continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
         os.unlink(self.path)
-        if sm:
-            out.update(sm_mhz=statistics.median(sm), sm_max_mhz=max(mx), reasons=sorted(reasons), samples=len(sm))
+        if self.t_begin is not None and self.t_end is not None:
+            inside = [r for r in rows if r[0] is not None and self.t_begin - 0.05 <= r[0] <= self.t_end + 0.05]
+            if inside:
+                rows = inside
+                out["window"] = "timed region"
+            else:
+                out["window"] = "whole sampling (no sample inside the timed region)"
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = {n for r in rows for n, v in zip(names, r[3]) if v.lower().startswith("active")}
+        if rows:
+            out.update(sm_mhz=statistics.median(r[1] for r in rows), sm_max_mhz=max(r[2] for r in rows),
+                       reasons=sorted(reasons), samples=len(rows))
         return out
 
 
@@ -166,6 +194,7 @@ def run_precision(lfts, precision, steps, warmup, rank, device, torch, clocks=No
     mix0 = s.anderson_stats()
     if clocks:
         clocks.start()
+        clocks.begin()
     ev0.record(stream)
     for i in range(warmup, nsteps_dev):
         k, _ = s.full_step_device(noise_dev[i].data_ptr(), CFG["max_iter"], CFG["tol"])
@@ -173,6 +202,8 @@ def run_precision(lfts, precision, steps, warmup, rank, device, torch, clocks=No
     ev1.record(stream)
     ev1.synchronize()
     torch.cuda.synchronize(device)
+    if clocks:
+        clocks.end()
     clk = clocks.stop() if clocks else None
     ms = ev0.elapsed_time(ev1) / steps
     launches = s.kernel_launches - launches0
