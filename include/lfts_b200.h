@@ -56,7 +56,7 @@ const char *lfts_version(void);
 const char *lfts_status_string(int status);
 /* text of the last CUDA error seen by any call in this process */
 const char *lfts_last_error_string(void);
-/* 1 when mesh dimension n has an FFT kernel in this build */
+/* 1 when mesh dimension n has an FFT kernel compiled into the library */
 int lfts_mesh_supported(int n);
 
 /* Allocates device state for one system: the diblock, step, anderson and
@@ -171,7 +171,7 @@ int lfts_get_propagators(lfts_ctx *ctx, double *q_host);
 
 
 /* ---- ensemble of independent replicas ------------------------------------ */
-/* Many independent FP32-mixed systems (BASELINE's batched configuration:
+/* Many independent FP32-mixed systems (the batched configuration:
  * replicas of different meshes, each with its own parameters and noise
  * stream) advanced together.  The reference runs one system per process;
  * there is no counterpart.  Each replica is a context of its own (buffers,

@@ -23,7 +23,7 @@ struct PencilKernels {
     int cw;
 };
 
-// false when (ny, nz) / nx has no instantiation in this build
+// false when (ny, nz) / nx has no compiled instantiation
 // packed-chain plane kernels (fft_packed.cuh), FP32
 bool plane_c_kernels(int ny, int nz, PlaneKernels<float> *out);
 // three-stage packed-chain plane kernels (fft_plane3.cuh), FP32: 64, 96, 128 square planes

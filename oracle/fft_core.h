@@ -1,7 +1,7 @@
 /*
  * TEST INFRASTRUCTURE ONLY -- part of the CPU oracle.  Nothing on the product
  * path may link or call this file; only tests/, the smoke check and the CPU
- * baseline leg of bench.py use it, as the checker.
+ * baseline leg of bench.py use it, as the oracle.
  *
  * Double-precision discrete Fourier transforms written from the DFT definition:
  *   forward  X[k] = sum_j x[j] exp(-2 pi i j k / n)

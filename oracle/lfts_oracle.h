@@ -2,7 +2,7 @@
  * TEST INFRASTRUCTURE ONLY -- the CPU oracle for the L-FTS diblock step.
  *
  * A plain-C restatement of tmbeardsley/lfts_cpu's hot path, used by tests/,
- * the smoke check and the CPU-baseline leg of bench.py as the checker.  The
+ * the smoke check and the CPU-baseline leg of bench.py as the oracle.  The
  * product (lfts_cpu_b200/) never links or calls it.  Each function cites the
  * reference lines it restates.  All arithmetic is FP64 like the reference.
  *

@@ -1,7 +1,7 @@
 """TEST INFRASTRUCTURE ONLY -- ctypes bindings for the CPU oracle.
 
 Imported only by tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg
-of ``bench.py``, as the checker.  The product package never imports it.
+of ``bench.py``, as the oracle.  The product package never imports it.
 
 * :class:`Oracle` wraps ``oracle/liblfts_oracle.so`` -- the plain-C restatement
   of the reference's hot path (``lfts_oracle.c``).
