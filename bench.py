@@ -173,7 +173,8 @@ def run_precision(lfts, precision, steps, warmup, rank, device, torch, clocks=No
     inp_sigma = np.sqrt(2.0 * M * CFG["dt"] / (CFG["C"] * np.prod(CFG["L"])))
     s = lfts.System(N, NA, CFG["XN"], CFG["C"], CFG["dt"], m, CFG["L"], precision=precision, device=device)
     rng = lfts.Rng(CFG["noise_seed"] + rank, inp_sigma)
-    s.langevin_init(rng.normal(M))
+    eta0 = rng.normal(M)
+    s.langevin_init(eta0)
     s.set_fields(make_initial_fields(M, CFG["field_seed"] + rank))
     s.mix(CFG["max_iter"], CFG["tol"])
     nsteps_dev = warmup + steps
@@ -186,6 +187,8 @@ def run_precision(lfts, precision, steps, warmup, rank, device, torch, clocks=No
     Ks = []
     for i in range(warmup):
         k, _ = s.full_step_device(noise_dev[i].data_ptr(), CFG["max_iter"], CFG["tol"])
+    # the state the timed steps start from, replayed by the end-to-end timing
+    snap = s.get_fields()[: 2 * M].copy() if do_e2e else None
     barrier(torch)
     torch.cuda.synchronize(device)
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -212,30 +215,40 @@ def run_precision(lfts, precision, steps, warmup, rank, device, torch, clocks=No
     res = {"ms_per_step": ms, "launches": launches, "iters": iters, "K": Ks, "clocks": clk,
            "calc_concs_per_step": iters / steps + 1.0}
     del noise_dev
-    # end to end through the C ABI with host (pinned) noise buffers
+    # End to end through the C ABI with host (pinned) noise buffers: after
+    # warm-up steps of its own, the context is put back into the state the
+    # device-resident timing started from (fields, previous noise, phi) and the
+    # same K steps are replayed from the same noise rows, now read from host
+    # memory.  The arithmetic is the same, so the Anderson counts repeat and
+    # the two timings differ only by the host-buffer API's transfers and syncs.
     if do_e2e:
-        host = torch.empty((warmup + steps, M), dtype=torch.float64, pin_memory=True)
-        for i in range(warmup + steps):
+        host = torch.empty((warmup, M), dtype=torch.float64, pin_memory=True)
+        for i in range(warmup):
             host[i].numpy()[:] = rng.normal(M)
         for i in range(warmup):
             s.langevin_step(host[i].numpy())
             s.mix(CFG["max_iter"], CFG["tol"])
             s.calc_concs()
+        s.set_fields(snap)
+        s.langevin_init(noise[warmup - 1].numpy() if warmup > 0 else eta0)
+        s.calc_concs()
         barrier(torch)
         torch.cuda.synchronize(device)
         mix0 = s.anderson_stats()
+        Ks_e2e = []
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for i in range(warmup, warmup + steps):
-            s.langevin_step(host[i].numpy())
-            s.mix(CFG["max_iter"], CFG["tol"])
+            s.langevin_step(noise[i].numpy())
+            Ks_e2e.append(s.mix(CFG["max_iter"], CFG["tol"]) - 1)
             s.calc_concs()
         e1.record(stream)
         e1.synchronize()
         mix1 = s.anderson_stats()
         it_e2e = mix1[1] - mix0[1]
         res["e2e_ms_per_step"] = e0.elapsed_time(e1) / steps
+        res["e2e_same_K"] = Ks_e2e == Ks
         res["h2d_bytes_per_step"] = 8 * M
         # per Anderson iteration S1 and <Dh0,Dh_m> (<= 11 doubles), plus Q and ln Q
         res["d2h_bytes_per_step"] = int(round((it_e2e / steps) * 8 * 11 + 16))
@@ -461,7 +474,9 @@ def main(argv=None):
             "data": "synthetic", "config": workload_config(),
             "e2e": {"value": world * 1e3 / e2e32, "unit": "steps/s",
                     "h2d_bytes_per_step": fp32["h2d_bytes_per_step"],
-                    "d2h_bytes_per_step": fp32["d2h_bytes_per_step"]},
+                    "d2h_bytes_per_step": fp32["d2h_bytes_per_step"],
+                    "steps": "the timed steps replayed from the same state and noise, noise read from pinned host memory",
+                    "same_anderson_K": fp32["e2e_same_K"]},
             "roofline": {"bound": "hbm", "kernel": "contour step (yz-plane + x-pencil kernels, both chains, FP32)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "traffic": traffic,
