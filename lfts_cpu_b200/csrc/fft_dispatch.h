@@ -10,14 +10,14 @@ namespace lfts {
 
 template <typename T>
 struct PlaneKernels {
-    void (*fn[4])(PlaneArgs<T>);  // indexed by PlaneMode
+    void (*fn[kPlaneModes])(PlaneArgs<T>);  // indexed by PlaneMode (null: not compiled)
     int nt;
     size_t smem;
 };
 
 template <typename T>
 struct PencilKernels {
-    void (*fn[2])(PencilArgs<T>);  // indexed by PencilMode
+    void (*fn[kPencilModes])(PencilArgs<T>);  // indexed by PencilMode (null: not compiled)
     int nt;
     size_t smem;
     int cw;

@@ -20,6 +20,7 @@ static void fill_plane(PlaneKernels<T> *o)
     o->fn[PLANE_INIT_Q] = plane_kernel<T, NY, NZ, PLANE_INIT_Q>;
     o->fn[PLANE_STEP] = plane_kernel<T, NY, NZ, PLANE_STEP>;
     o->fn[PLANE_LAST] = plane_kernel<T, NY, NZ, PLANE_LAST>;
+    o->fn[PLANE_G] = nullptr;
     o->nt = C::NT;
     o->smem = C::SMEM;
 }
@@ -32,6 +33,7 @@ static void fill_plane_c(PlaneKernels<T> *o)
     o->fn[PLANE_INIT_Q] = plane_c_kernel<T, NY, NZ, PLANE_INIT_Q>;
     o->fn[PLANE_STEP] = plane_c_kernel<T, NY, NZ, PLANE_STEP>;
     o->fn[PLANE_LAST] = plane_c_kernel<T, NY, NZ, PLANE_LAST>;
+    o->fn[PLANE_G] = nullptr;
     o->nt = C::NT;
     o->smem = C::SMEM;
 }
@@ -46,6 +48,14 @@ static void fill_pencil(PencilKernels<T> *o)
         o->fn[PENCIL_POWER] = pencil_kernel<T, NX, CW, PENCIL_POWER>;
     else
         o->fn[PENCIL_POWER] = nullptr;
+    // the h-in-pencil chain: FP32 packed field, 128-point x lines
+    if constexpr (sizeof(T) == sizeof(float) && NX == 128) {
+        o->fn[PENCIL_H] = pencil_kernel<T, NX, CW, PENCIL_H>;
+        o->fn[PENCIL_H_LAST] = pencil_kernel<T, NX, CW, PENCIL_H_LAST>;
+        o->fn[PENCIL_INIT_W] = pencil_kernel<T, NX, CW, PENCIL_INIT_W>;
+    } else {
+        o->fn[PENCIL_H] = o->fn[PENCIL_H_LAST] = o->fn[PENCIL_INIT_W] = nullptr;
+    }
     o->nt = C::NT;
     o->smem = C::SMEM;
     o->cw = CW;

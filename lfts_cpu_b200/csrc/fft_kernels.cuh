@@ -41,7 +41,9 @@ enum PlaneMode : int {
     PLANE_INIT_Q = 1,  // forward transform of given real rows (q_in or W-)
     PLANE_STEP = 2,    // inverse, x h, store q, forward
     PLANE_LAST = 3,    // inverse, x h, store q, partial sum of chain 0 (for Q)
+    PLANE_G = 4,       // inverse, x g (separable tables), forward; stores nothing
 };
+constexpr int kPlaneModes = 5;
 
 template <typename T>
 struct PlaneArgs {
@@ -58,6 +60,7 @@ struct PlaneArgs {
     int cbase;            // chain index of blockIdx.y == 0 (one-chain launches)
     int nchains;
     double Nd;            // N as a double (h = exp(-w/N))
+    const T *gx, *gy, *gz;  // PLANE_G: separable Boltzmann weight, 1/M folded into gz
 };
 
 template <typename T, int NY, int NZ>
@@ -647,9 +650,14 @@ __global__ void __launch_bounds__(PlaneCfg<T, NY, NZ>::NT, PlaneCfg<T, NY, NZ>::
 
 // ----------------------------------------------------------- pencil kernel --
 enum PencilMode : int {
-    PENCIL_CONV = 0,  // forward x, times g, inverse x (in place in the spectrum)
-    PENCIL_POWER = 1, // forward x, S += |X|^2 (structure function sample)
+    PENCIL_CONV = 0,    // forward x, times g, inverse x (in place in the spectrum)
+    PENCIL_POWER = 1,   // forward x, S += |X|^2 (structure function sample)
+    // the h-in-pencil chain (FP32 packed field): see enqueue_chain_launches
+    PENCIL_H = 2,       // forward x, times h, store q, inverse x
+    PENCIL_H_LAST = 3,  // forward x, times h, store q
+    PENCIL_INIT_W = 4,  // h = exp(-w/N) from the fields, store it, inverse x
 };
+constexpr int kPencilModes = 5;
 
 template <typename T>
 struct PencilArgs {
@@ -660,6 +668,13 @@ struct PencilArgs {
     int ncol;                 // my*KZ
     int KZ;
     int cbase;                // chain index of blockIdx.y == 0
+    // PENCIL_H, PENCIL_H_LAST, PENCIL_INIT_W (packed field: (chain 1, chain 2) pairs)
+    const double *w;          // INIT_W: W- (M) and w+ (M), FP64
+    const T *h;               // (hA, hB) pairs
+    T *qout;                  // stored propagators (pairs), or h for INIT_W
+    int hsel0, hsel1;         // h half used by chain 1 / chain 2 (0 = hA, 1 = hB)
+    long long M;
+    double Nd;                // N as a double (h = exp(-w/N))
 };
 
 template <typename T, int NX, int CW>
@@ -702,7 +717,7 @@ __device__ __forceinline__ void pencil_body(const PencilArgs<T> &a, const int ti
     // most one task per thread (CW * R2 <= NT); its loads go out before the
     // barrier that publishes the tables.
     static_assert(CW * R2 <= C::NT, "one stage-A task per thread");
-    {
+    if (MODE != PENCIL_INIT_W) {
         const int t = threadIdx.x;
         const int cl = t % CW, j2 = t / CW, col = col0 + cl;
         const bool act = t < CW * R2 && col < ncol;
@@ -720,14 +735,50 @@ __device__ __forceinline__ void pencil_body(const PencilArgs<T> &a, const int ti
     }
     __syncthreads();
 
-    // X2: forward stage B -> X[k1 + R1 k2]; then g and inverse stage B, or |X|^2
+    // X2: forward stage B -> X[k1 + R1 k2]; then g and inverse stage B, or |X|^2.
+    // The h modes see the forward transform of their input at real-space x =
+    // k1 + R1 k2 (the chain that uses them is written out at
+    // enqueue_chain_launches); INIT_W starts from h at those points.
     for (int t = threadIdx.x; t < CW * R1; t += C::NT) {
         const int cl = t % CW, k1 = t / CW, col = col0 + cl;
         if (col >= ncol) continue;
         cpx<T> v[R2];
+        if constexpr (MODE == PENCIL_INIT_W) {
+            // hA = exp(-(W- + w+)/N), hB = exp(-(-W- + w+)/N)  (src/diblock.cc:64-72),
+            // single-precision exponential as the FP32 plane kernels' INIT_W
+            static_assert(sizeof(T) == sizeof(float), "FP32 packed field only");
 #pragma unroll
-        for (int u = 0; u < R2; u++) v[u] = Tl[C::row(R2 * k1 + u) * CW + cl];
-        Dft<R2, -1, T>::run(v);
+            for (int k2 = 0; k2 < R2; k2++) {
+                const long long o = (long long)(k1 + R1 * k2) * ncol + col;
+                const double wm = a.w[o], wp = a.w[a.M + o];
+                const float v1 = expf((float)(-(wm + wp) / a.Nd));
+                const float v2 = expf((float)(-(-wm + wp) / a.Nd));
+                reinterpret_cast<cpx<float> *>(a.qout)[o] = {v1, v2};
+                v[k2] = {v1, v2};
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < R2; u++) v[u] = Tl[C::row(R2 * k1 + u) * CW + cl];
+            Dft<R2, -1, T>::run(v);
+        }
+        if constexpr (MODE == PENCIL_H || MODE == PENCIL_H_LAST) {
+            static_assert(sizeof(T) == sizeof(float), "FP32 packed field only");
+            const int hs0 = a.hsel0, hs1 = a.hsel1;
+#pragma unroll
+            for (int k2 = 0; k2 < R2; k2++) {
+                const long long o = (long long)(k1 + R1 * k2) * ncol + col;
+                const float2 h = __ldg(reinterpret_cast<const float2 *>(a.h) + o);
+                const float va = v[k2].x * (hs0 ? h.y : h.x);
+                const float vb = v[k2].y * (hs1 ? h.y : h.x);
+                __stcs(reinterpret_cast<float2 *>(a.qout) + o, make_float2(va, vb));
+                v[k2] = {va, vb};
+            }
+        }
+        if constexpr (MODE == PENCIL_H || MODE == PENCIL_INIT_W) {
+            Dft<R2, 1, T>::run(v);
+#pragma unroll
+            for (int u = 0; u < R2; u++) Tl[C::row(R2 * k1 + u) * CW + cl] = ctw<1>(v[u], twx[(u * k1) % NX]);
+        }
         if (MODE == PENCIL_CONV) {
             const T gyz = a.gy[col / a.KZ] * a.gz[col % a.KZ];
 #pragma unroll
@@ -735,7 +786,7 @@ __device__ __forceinline__ void pencil_body(const PencilArgs<T> &a, const int ti
             Dft<R2, 1, T>::run(v);
 #pragma unroll
             for (int u = 0; u < R2; u++) Tl[C::row(R2 * k1 + u) * CW + cl] = ctw<1>(v[u], twx[(u * k1) % NX]);
-        } else {
+        } else if (MODE == PENCIL_POWER) {
 #pragma unroll
             for (int k2 = 0; k2 < R2; k2++) {
                 const long long o = (long long)(k1 + R1 * k2) * ncol + col;
@@ -743,7 +794,7 @@ __device__ __forceinline__ void pencil_body(const PencilArgs<T> &a, const int ti
             }
         }
     }
-    if (MODE == PENCIL_POWER) return;
+    if (MODE == PENCIL_POWER || MODE == PENCIL_H_LAST) return;
     __syncthreads();
 
     // X3: inverse stage A (strided) -> natural order, to global

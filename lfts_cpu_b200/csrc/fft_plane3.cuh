@@ -179,8 +179,11 @@ __device__ __forceinline__ void p3_s2_fwd(cpx<float> *P, const cpx<float> *TY, c
 }
 
 // S3 tasks: (y, c1) = (u / Z1, u % Z1) for u = threadIdx.x + NT s, s < ROUNDS
+// MODE PLANE_G multiplies by the Boltzmann weight g = gx[x] (gy[y] gz[z]) of
+// plane x instead of h and stores nothing (the h-in-pencil chain)
 template <typename C, int MODE>
-__device__ __forceinline__ void p3_s3(cpx<float> *P, const PlaneArgs<float> &a, long long plane_off, double &qsum)
+__device__ __forceinline__ void p3_s3(cpx<float> *P, const PlaneArgs<float> &a, long long plane_off, double &qsum,
+                                      int x)
 {
     constexpr int NZ = C::NZ, Z1 = C::Z1, Z2 = C::Z2;
     // stored propagators and h as (chain 1, chain 2) pairs (fft_packed.cuh)
@@ -195,11 +198,17 @@ __device__ __forceinline__ void p3_s3(cpx<float> *P, const PlaneArgs<float> &a, 
         const int y = u / Z1, c1 = u % Z1;
         cpx<float> *row = P + y * C::KP;
         float ha[Z2], hb[Z2];
+        if (MODE == PLANE_G) {
+            const float gx = __ldg(a.gx + x), gy = __ldg(a.gy + y);
 #pragma unroll
-        for (int c2 = 0; c2 < Z2; c2++) {
-            const cpx<float> h = ld_pair(hp + y * NZ + c1 + Z1 * c2);
-            ha[c2] = hs0 ? h.y : h.x;
-            hb[c2] = hs1 ? h.y : h.x;
+            for (int c2 = 0; c2 < Z2; c2++) ha[c2] = hb[c2] = gx * (gy * __ldg(a.gz + c1 + Z1 * c2));
+        } else {
+#pragma unroll
+            for (int c2 = 0; c2 < Z2; c2++) {
+                const cpx<float> h = ld_pair(hp + y * NZ + c1 + Z1 * c2);
+                ha[c2] = hs0 ? h.y : h.x;
+                hb[c2] = hs1 ? h.y : h.x;
+            }
         }
         cpx<float> g[Z2];
         p3_ld16(row + C::pos(Z2 * c1), g);
@@ -209,11 +218,11 @@ __device__ __forceinline__ void p3_s3(cpx<float> *P, const PlaneArgs<float> &a, 
             const int z = c1 + Z1 * c2;
             const float va = g[c2].x * ha[c2];
             const float vb = g[c2].y * hb[c2];
-            st_pair(qp + y * NZ + z, va, vb);
+            if (MODE != PLANE_G) st_pair(qp + y * NZ + z, va, vb);
             if (MODE == PLANE_LAST) qsum += (double)va;
             g[c2] = {va, vb};
         }
-        if (MODE == PLANE_STEP) {
+        if (MODE == PLANE_STEP || MODE == PLANE_G) {
             Dft<Z2, -1, float>::run(g);
             p3_st16(row + C::pos(Z2 * c1), g);
         }
@@ -296,7 +305,7 @@ __device__ __forceinline__ void plane3_body(const PlaneArgs<float> &a, const int
     p3_s2_inv<C>(P, TY, TZ);
     __syncthreads();
     double qsum = 0.0;
-    p3_s3<C, MODE>(P, a, plane_off, qsum);
+    p3_s3<C, MODE>(P, a, plane_off, qsum, x);
     if (MODE == PLANE_LAST) {
         __shared__ double red[C::NT / 32];
         for (int o = 16; o > 0; o >>= 1) qsum += __shfl_xor_sync(0xffffffffu, qsum, o);

@@ -54,6 +54,20 @@ static __global__ void q_finalize_kernel(const double *qpart, int n, long long M
     }
 }
 
+// Per-plane sums of chain 1's last propagator q_N (the first component of the
+// stored FP32 pairs), one CTA per x-plane in a fixed order: the partials
+// q_finalize_kernel reduces, for the chain that stores q in the x-pencil.
+static __global__ void __launch_bounds__(256) plane_q_sums_kernel(const float2 *__restrict__ qN, long long plane,
+                                                                  double *qpart)
+{
+    __shared__ double sh[32];
+    const float2 *p = qN + blockIdx.x * plane;
+    double s = 0.0;
+    for (long long i = threadIdx.x; i < plane; i += blockDim.x) s += (double)p[i].x;
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) qpart[blockIdx.x] = s;
+}
+
 template <typename T, int V>
 struct VecOf;
 template <> struct VecOf<float, 4> { using type = float4; };

@@ -121,9 +121,9 @@ PencilKernels<float> &pencil_of<float>(lfts_ctx *c) { return c->pe32; }
 template <typename T>
 int set_smem_attrs(const PlaneKernels<T> &pl, const PencilKernels<T> &pe)
 {
-    for (int m = 0; m < 4; m++)
-        CK(cudaFuncSetAttribute(pl.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
-    for (int m = 0; m < 2; m++)
+    for (int m = 0; m < kPlaneModes; m++)
+        if (pl.fn[m]) CK(cudaFuncSetAttribute(pl.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
+    for (int m = 0; m < kPencilModes; m++)
         if (pe.fn[m]) CK(cudaFuncSetAttribute(pe.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pe.smem));
     return LFTS_OK;
 }
@@ -175,6 +175,9 @@ PlaneArgs<T> plane_args(lfts_ctx *c)
     a.qpart = c->qpart;
     a.nchains = 2;
     a.Nd = (double)c->N;
+    a.gx = static_cast<const T *>(c->gtab[0]);
+    a.gy = static_cast<const T *>(c->gtab[1]);
+    a.gz = static_cast<const T *>(c->gtab[2]);
     return a;
 }
 
@@ -189,6 +192,10 @@ PencilArgs<T> pencil_args(lfts_ctx *c)
     a.gz = static_cast<const T *>(c->gtab[2]);
     a.ncol = c->my * (c->packed ? c->mz : c->KZ);
     a.KZ = c->packed ? c->mz : c->KZ;
+    a.w = c->w;
+    a.h = static_cast<const T *>(c->q);  // slot 1: the (hA, hB) pairs
+    a.M = c->M;
+    a.Nd = (double)c->N;
     return a;
 }
 
@@ -294,6 +301,34 @@ void enqueue_chain_launches(lfts_ctx *c)
     const long long M = c->M;
     PlaneArgs<T> a = plane_args<T>(c);
     PencilArgs<T> pa = pencil_args<T>(c);
+    if constexpr (sizeof(T) == sizeof(float)) {
+        if (c->xh_chain) {
+            // One step is q_{i+1} = h . F^-1[g . F[q_i]].  g is even in every
+            // wavenumber, so F^-1[g F[q]] = F[g F^-1[q]]; with D_i = F_x^-1[q_i]
+            // in the spectrum buffer a step is
+            //   yz-plane (PLANE_G):  E_i = F_yz[g . F_yz^-1[D_i]]  (the STEP flow, g for h)
+            //   x-pencil (PENCIL_H): q_{i+1} = h . F_x[E_i], stored; D_{i+1} = F_x^-1[q_{i+1}]
+            // which puts the h loads and q stores in the pencil's several CTAs
+            // per SM instead of the plane kernel's one.
+            PencilArgs<T> pi = pa;
+            pi.qout = q;  // slot 1 = (hA, hB)
+            launch_pencil<T>(c, PENCIL_INIT_W, pi, 2);
+            for (int i = 1; i < c->N; i++) {
+                launch_plane<T>(c, PLANE_G, a, 2);
+                PencilArgs<T> ph = pa;
+                ph.qout = q + (long long)i * 2 * M;  // slot i+1
+                ph.hsel0 = hsel_chain0(c, i);
+                ph.hsel1 = hsel_chain1(c, i);
+                launch_pencil<T>(c, i + 1 < c->N ? PENCIL_H : PENCIL_H_LAST, ph, 2);
+            }
+            plane_q_sums_kernel<<<c->mx, 256, 0, c->st>>>(
+                reinterpret_cast<const float2 *>(q + (long long)(c->N - 1) * 2 * M), (long long)c->my * c->mz,
+                c->qpart);
+            q_finalize_kernel<<<1, 256, 0, c->st>>>(c->qpart, c->mx, M, c->Qd);
+            c->launches += 2;
+            return;
+        }
+    }
     if (!c->two_streams || c->packed) {
         a.qout = q;  // slot 1 = [hA | hB]
         launch_plane<T>(c, PLANE_INIT_W, a, 2);
@@ -369,7 +404,7 @@ int set_pencil(lfts_ctx *c, int cw)
 {
     PencilKernels<T> pk{};
     if (!pencil_kernels(c->mx, cw, &pk)) return LFTS_ERR_UNSUPPORTED;
-    for (int m = 0; m < 2; m++)
+    for (int m = 0; m < kPencilModes; m++)
         if (pk.fn[m]) CK(cudaFuncSetAttribute(pk.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pk.smem));
     pencil_of<T>(c) = pk;
     return LFTS_OK;
@@ -441,34 +476,63 @@ int profile_chain(lfts_ctx *c, double *ms_plane, double *ms_pencil, double *ms_c
     T *q = static_cast<T *>(c->q);
     const long long M = c->M;
     PlaneArgs<T> a = plane_args<T>(c);
-    a.qout = q;
-    CK(cudaEventRecord(ev[4 * n], c->st));
-    launch_plane<T>(c, PLANE_INIT_W, a, 2);
     PencilArgs<T> pa = pencil_args<T>(c);
-    a.h = q;
-    for (int i = 1; i < c->N; i++) {
-        const int j = i - 1;
-        CK(cudaEventRecord(ev[4 * j], c->st));
-        launch_pencil<T>(c, PENCIL_CONV, pa, 2);
-        CK(cudaEventRecord(ev[4 * j + 1], c->st));
-        a.qout = q + (long long)i * 2 * M;
-        a.hsel0 = hsel_chain0(c, i);
-        a.hsel1 = hsel_chain1(c, i);
-        CK(cudaEventRecord(ev[4 * j + 2], c->st));
-        launch_plane<T>(c, i + 1 < c->N ? PLANE_STEP : PLANE_LAST, a, 2);
-        CK(cudaEventRecord(ev[4 * j + 3], c->st));
+    // per step j: pencil between ev[4j] and ev[4j+1], plane between ev[4j+2] and ev[4j+3]
+    CK(cudaEventRecord(ev[4 * n], c->st));
+    if (c->xh_chain) {
+        // the chain of enqueue_chain_launches: pencil INIT_W, (N-1) x (plane G, pencil H)
+        PencilArgs<T> pi = pa;
+        pi.qout = q;
+        launch_pencil<T>(c, PENCIL_INIT_W, pi, 2);
+        for (int i = 1; i < c->N; i++) {
+            const int j = i - 1;
+            CK(cudaEventRecord(ev[4 * j + 2], c->st));
+            launch_plane<T>(c, PLANE_G, a, 2);
+            CK(cudaEventRecord(ev[4 * j + 3], c->st));
+            PencilArgs<T> ph = pa;
+            ph.qout = q + (long long)i * 2 * M;
+            ph.hsel0 = hsel_chain0(c, i);
+            ph.hsel1 = hsel_chain1(c, i);
+            CK(cudaEventRecord(ev[4 * j], c->st));
+            launch_pencil<T>(c, i + 1 < c->N ? PENCIL_H : PENCIL_H_LAST, ph, 2);
+            CK(cudaEventRecord(ev[4 * j + 1], c->st));
+        }
+        if constexpr (sizeof(T) == sizeof(float))
+            plane_q_sums_kernel<<<c->mx, 256, 0, c->st>>>(
+                reinterpret_cast<const float2 *>(q + (long long)(c->N - 1) * 2 * M), (long long)c->my * c->mz,
+                c->qpart);
+    } else {
+        a.qout = q;
+        launch_plane<T>(c, PLANE_INIT_W, a, 2);
+        a.h = q;
+        for (int i = 1; i < c->N; i++) {
+            const int j = i - 1;
+            CK(cudaEventRecord(ev[4 * j], c->st));
+            launch_pencil<T>(c, PENCIL_CONV, pa, 2);
+            CK(cudaEventRecord(ev[4 * j + 1], c->st));
+            a.qout = q + (long long)i * 2 * M;
+            a.hsel0 = hsel_chain0(c, i);
+            a.hsel1 = hsel_chain1(c, i);
+            CK(cudaEventRecord(ev[4 * j + 2], c->st));
+            launch_plane<T>(c, i + 1 < c->N ? PLANE_STEP : PLANE_LAST, a, 2);
+            CK(cudaEventRecord(ev[4 * j + 3], c->st));
+        }
     }
     q_finalize_kernel<<<1, 256, 0, c->st>>>(c->qpart, c->mx, M, c->Qd);
-    c->launches++;
+    c->launches += c->xh_chain ? 2 : 1;
     CK(cudaEventRecord(ev[4 * n + 1], c->st));
     CK(cudaEventSynchronize(ev[4 * n + 1]));
+    // means over the full-step launches (the last step's short launch left out)
     double pl = 0.0, pe = 0.0;
-    int npl = 0;
+    int npl = 0, npe = 0;
     for (int j = 0; j < n; j++) {
         float t = 0.f;
-        CK(cudaEventElapsedTime(&t, ev[4 * j], ev[4 * j + 1]));
-        pe += t;
-        if (j + 1 < n) {
+        if (j + 1 < n || !c->xh_chain) {
+            CK(cudaEventElapsedTime(&t, ev[4 * j], ev[4 * j + 1]));
+            pe += t;
+            npe++;
+        }
+        if (j + 1 < n || c->xh_chain) {
             CK(cudaEventElapsedTime(&t, ev[4 * j + 2], ev[4 * j + 3]));
             pl += t;
             npl++;
@@ -482,7 +546,7 @@ int profile_chain(lfts_ctx *c, double *ms_plane, double *ms_pencil, double *ms_c
     float tc = 0.f;
     CK(cudaEventElapsedTime(&tc, ev[0], ev[1]));
     for (auto &e : ev) cudaEventDestroy(e);
-    *ms_pencil = pe / n;
+    *ms_pencil = npe ? pe / npe : 0.0;
     *ms_plane = npl ? pl / npl : 0.0;
     *ms_chain = tc;
     return LFTS_OK;
@@ -951,6 +1015,10 @@ int lfts_create(const lfts_params *p, int precision, int device, lfts_ctx **out)
         else if (!plane_c_kernels(c->my, c->mz, &c->pl32))
             return fail(LFTS_ERR_UNSUPPORTED);
         if (!pencil_kernels(c->mx, kDefaultCwFp32, &c->pe32)) return fail(LFTS_ERR_UNSUPPORTED);
+        // h and the stored propagators in the x-pencil where both kernels have
+        // those modes (128^3); LFTS_XH_CHAIN=0 keeps them in the yz-plane kernel
+        const char *xh = getenv("LFTS_XH_CHAIN");
+        c->xh_chain = c->pl32.fn[PLANE_G] && c->pe32.fn[PENCIL_H] && !(xh && xh[0] == '0');
         if ((rc = set_smem_attrs(c->pl32, c->pe32))) return fail(rc);
     }
     if ((rc = ctx_alloc(c))) return fail(rc == LFTS_ERR_CUDA ? LFTS_ERR_NOMEM : rc);

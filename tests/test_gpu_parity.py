@@ -4,6 +4,8 @@ larger meshes, and size-independent identities at the full 128^3, N=64 size.
 
 Tolerances: FP64 path 1e-10 relative (the bar the reference is held to);
 FP32-mixed path 1e-5 on phi."""
+import os
+
 import numpy as np
 import pytest
 
@@ -200,6 +202,36 @@ def test_full_size_identities_128(lfts, precision):
         s64.set_fields(w2)
         s64.calc_concs()
         assert rel_err(w[2 * M:], s64.get_fields()[2 * M:]) < FP32_PHI_TOL
+
+
+def test_fp32_chain_with_h_in_pencil_128(lfts):
+    """At 128^3 the FP32-mixed chain applies h and stores the propagators in
+    the x-pencil kernel and g in the yz-plane kernel (exact because g is even
+    in every wavenumber).  The same fields through the chain that keeps h in
+    the yz-plane kernel (LFTS_XH_CHAIN=0) give the same ln Q, phi and
+    propagators to the FP32 tolerance."""
+    m, N, NA = (128, 128, 128), 8, 3
+    M = int(np.prod(m))
+    w2 = np.random.default_rng(11).normal(0.0, 0.5, 2 * M)
+    out = []
+    for flag in ("1", "0"):
+        old = os.environ.get("LFTS_XH_CHAIN")
+        os.environ["LFTS_XH_CHAIN"] = flag
+        try:
+            s = lfts.System(N, NA, 16.0, 100.0, 0.5, m, (8.0, 8.0, 8.0), precision=1)
+        finally:
+            if old is None:
+                del os.environ["LFTS_XH_CHAIN"]
+            else:
+                os.environ["LFTS_XH_CHAIN"] = old
+        s.set_fields(w2)
+        lnq = s.calc_concs()
+        out.append((lnq, s.get_fields()[2 * M:], s.propagators().ravel()))
+        s.close()
+    (lnq_a, phi_a, q_a), (lnq_b, phi_b, q_b) = out
+    assert abs(lnq_a - lnq_b) < FP32_PHI_TOL * max(1.0, abs(lnq_b))
+    assert rel_err(phi_a, phi_b) < FP32_PHI_TOL
+    assert rel_err(q_a, q_b) < FP32_PHI_TOL
 
 
 @pytest.mark.parametrize("name", ["comp_16", "comp_12x24x16"])
