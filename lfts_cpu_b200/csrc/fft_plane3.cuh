@@ -37,10 +37,11 @@ struct Plane3Cfg {
     static constexpr int NS1 = NZ * Y2, NS2 = Y1 * Z2, NS3 = NY * Z1;  // tasks per stage
     // TY[j2 * Y1 + k1] = w^(j2 k1) (NY entries), TZ[c1 * Z2 + jz] = w^(jz c1) (NZ entries)
     static constexpr size_t TOFF = sizeof(cpx<float>) * (size_t)(NY * KP);
-    static constexpr size_t SMEM = TOFF + sizeof(cpx<float>) * (NY + NZ);
+    // ... followed by gz[NZ] (PLANE_G)
+    static constexpr size_t SMEM = TOFF + sizeof(cpx<float>) * (NY + NZ) + sizeof(float) * NZ;
     static __host__ __device__ constexpr int pos(int p) { return p + 2 * (p / Z2); }
     static_assert(Z2 == 16, "S3 runs of 16 values");
-    static_assert(NS1 <= NT && NS2 <= NT && NY + NZ <= NT, "at most one S1 / S2 task per thread");
+    static_assert(NS1 <= NT && NS2 <= NT && NY + 2 * NZ <= NT, "at most one S1 / S2 task (table entry) per thread");
     static_assert(pos(NZ - 1) < KP && KP % 2 == 0, "row pitch");
 };
 
@@ -183,7 +184,7 @@ __device__ __forceinline__ void p3_s2_fwd(cpx<float> *P, const cpx<float> *TY, c
 // plane x instead of h and stores nothing (the h-in-pencil chain)
 template <typename C, int MODE>
 __device__ __forceinline__ void p3_s3(cpx<float> *P, const PlaneArgs<float> &a, long long plane_off, double &qsum,
-                                      int x)
+                                      int x, const float *GZ)
 {
     constexpr int NZ = C::NZ, Z1 = C::Z1, Z2 = C::Z2;
     // stored propagators and h as (chain 1, chain 2) pairs (fft_packed.cuh)
@@ -201,7 +202,7 @@ __device__ __forceinline__ void p3_s3(cpx<float> *P, const PlaneArgs<float> &a, 
         if (MODE == PLANE_G) {
             const float gx = __ldg(a.gx + x), gy = __ldg(a.gy + y);
 #pragma unroll
-            for (int c2 = 0; c2 < Z2; c2++) ha[c2] = hb[c2] = gx * (gy * __ldg(a.gz + c1 + Z1 * c2));
+            for (int c2 = 0; c2 < Z2; c2++) ha[c2] = hb[c2] = gx * (gy * GZ[c1 + Z1 * c2]);
         } else {
 #pragma unroll
             for (int c2 = 0; c2 < Z2; c2++) {
@@ -275,6 +276,7 @@ __device__ __forceinline__ void plane3_body(const PlaneArgs<float> &a, const int
     cpx<float> *P = reinterpret_cast<cpx<float> *>(smem_raw);
     cpx<float> *TY = reinterpret_cast<cpx<float> *>(smem_raw + C::TOFF);
     cpx<float> *TZ = TY + C::NY;
+    float *GZ = reinterpret_cast<float *>(TZ + C::NZ);
 
     const long long M = (long long)mx * C::NY * C::NZ;
     const long long plane_off = (long long)x * C::NY * C::NZ;
@@ -287,6 +289,8 @@ __device__ __forceinline__ void plane3_body(const PlaneArgs<float> &a, const int
     } else if (threadIdx.x < C::NY + C::NZ) {
         const int t = threadIdx.x - C::NY, c1 = t / C::Z2, jz = t % C::Z2;
         TZ[t] = a.twz[(jz * c1) % C::NZ];
+    } else if (MODE == PLANE_G && threadIdx.x < C::NY + 2 * C::NZ) {
+        GZ[threadIdx.x - C::NY - C::NZ] = a.gz[threadIdx.x - C::NY - C::NZ];
     }
     pdl_launch_dependents();
     pdl_wait();
@@ -305,7 +309,7 @@ __device__ __forceinline__ void plane3_body(const PlaneArgs<float> &a, const int
     p3_s2_inv<C>(P, TY, TZ);
     __syncthreads();
     double qsum = 0.0;
-    p3_s3<C, MODE>(P, a, plane_off, qsum, x);
+    p3_s3<C, MODE>(P, a, plane_off, qsum, x, GZ);
     if (MODE == PLANE_LAST) {
         __shared__ double red[C::NT / 32];
         for (int o = 16; o > 0; o >>= 1) qsum += __shfl_xor_sync(0xffffffffu, qsum, o);
