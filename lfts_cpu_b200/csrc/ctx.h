@@ -22,6 +22,7 @@ struct lfts_ctx {
     cudaStream_t st = nullptr;
     cudaStream_t st1 = nullptr;         // chain 1 of the contour chain runs here
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_h[2] = {};  // each chain's half of h written (two-stream FP64 chain)
     int sms = 148;
 
     double *w = nullptr;       // 4M: W-, w+, phi-, phi+

@@ -262,8 +262,6 @@ void enqueue_chain(lfts_ctx *c)
                 c->chain_graph = g;
                 c->chain_kernels = c->launches - before;
                 // upload before the first replay and let both streams drain
-                // (the first replay after a two-stream capture misordered
-                // without this on B200 / driver 580)
                 e = cudaGraphUpload(c->chain_exec, c->st);
                 if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
                 if (e == cudaSuccess) e = cudaStreamSynchronize(c->st1);
@@ -353,6 +351,12 @@ void enqueue_chain_launches(lfts_ctx *c)
             launch_plane<T>(c, PLANE_INIT_W, ac[k], 1, sc[k]);
             ac[k].h = q;
         }
+        // Each stream's INIT_W writes its own half of h (hA from chain 1, hB from
+        // chain 2), and each chain's steps read the other half once i >= NA
+        // (chain 1) or i >= NB (chain 2): both halves are complete before either
+        // chain's first step.
+        for (int k = 0; k < 2; k++) cudaEventRecord(c->ev_h[k], sc[k]);
+        for (int k = 0; k < 2; k++) cudaStreamWaitEvent(sc[k], c->ev_h[1 - k], 0);
         for (int i = 1; i < c->N; i++) {
             for (int k = 0; k < 2; k++) launch_pencil<T>(c, PENCIL_CONV, pc[k], 1, sc[k]);
             for (int k = 0; k < 2; k++) {
@@ -781,6 +785,8 @@ void ctx_free(lfts_ctx *c)
     if (c->st1) cudaStreamSynchronize(c->st1);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
+    for (int k = 0; k < 2; k++)
+        if (c->ev_h[k]) cudaEventDestroy(c->ev_h[k]);
     if (c->st1) cudaStreamDestroy(c->st1);
     if (c->st) cudaStreamDestroy(c->st);
 }
@@ -1004,7 +1010,9 @@ int lfts_create(const lfts_params *p, int precision, int device, lfts_ctx **out)
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->st1, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_h[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_h[1], cudaEventDisableTiming) != cudaSuccess)
         return fail(LFTS_ERR_CUDA);
     if (!plane_kernels(c->my, c->mz, &c->pl64) || !pencil_kernels(c->mx, &c->pe64)) return fail(LFTS_ERR_UNSUPPORTED);
     if ((rc = set_smem_attrs(c->pl64, c->pe64))) return fail(rc);
