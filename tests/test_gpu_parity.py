@@ -204,13 +204,15 @@ def test_full_size_identities_128(lfts, precision):
         assert rel_err(w[2 * M:], s64.get_fields()[2 * M:]) < FP32_PHI_TOL
 
 
-def test_fp32_chain_with_h_in_pencil_128(lfts):
+@pytest.mark.parametrize("N,NA", [(8, 3), (2, 1), (3, 0), (4, 4)])
+def test_fp32_chain_with_h_in_pencil_128(lfts, N, NA):
     """At 128^3 the FP32-mixed chain applies h and stores the propagators in
     the x-pencil kernel and g in the yz-plane kernel (exact because g is even
     in every wavenumber).  The same fields through the chain that keeps h in
     the yz-plane kernel (LFTS_XH_CHAIN=0) give the same ln Q, phi and
-    propagators to the FP32 tolerance."""
-    m, N, NA = (128, 128, 128), 8, 3
+    propagators to the FP32 tolerance; N = 2 (one step: the last pencil right
+    after INIT_W) and pure-B / pure-A chains included."""
+    m = (128, 128, 128)
     M = int(np.prod(m))
     w2 = np.random.default_rng(11).normal(0.0, 0.5, 2 * M)
     out = []
