@@ -176,7 +176,9 @@ int lfts_get_propagators(lfts_ctx *ctx, double *q_host);
  * stream) advanced together.  The reference runs one system per process;
  * there is no counterpart.  Each replica is a context of its own (buffers,
  * tables, autotuned x-pencil width), computes exactly what a single
- * FP32-mixed context computes when fed the same noise, and the ensemble
+ * FP32-mixed context computes when fed the same noise (at 96^3 a context
+ * created with LFTS_XH_CHAIN=0 in the environment: the ensemble keeps h in the
+ * yz-plane kernel, single 96^3 contexts default to the x-pencil), and the ensemble
  * captures one Langevin step of every replica -- update, Anderson loop with
  * the least squares on the device, the extra calc_concs -- as one CUDA graph
  * launch (a WHILE node runs until every replica's loop has ended).

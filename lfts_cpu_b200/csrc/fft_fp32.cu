@@ -28,8 +28,8 @@ static void fill_plane3(PlaneKernels<float> *o)
     o->fn[PLANE_INIT_Q] = plane3_kernel<C, PLANE_INIT_Q>;
     o->fn[PLANE_STEP] = plane3_kernel<C, PLANE_STEP>;
     o->fn[PLANE_LAST] = plane3_kernel<C, PLANE_LAST>;
-    // the h-in-pencil chain runs on 128 x 128 planes
-    if constexpr (C::NY == 128)
+    // the h-in-pencil chain runs on 96 x 96 and 128 x 128 planes
+    if constexpr (C::NY == 96 || C::NY == 128)
         o->fn[PLANE_G] = plane3_kernel<C, PLANE_G>;
     else
         o->fn[PLANE_G] = nullptr;

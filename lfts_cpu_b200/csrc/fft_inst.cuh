@@ -48,8 +48,9 @@ static void fill_pencil(PencilKernels<T> *o)
         o->fn[PENCIL_POWER] = pencil_kernel<T, NX, CW, PENCIL_POWER>;
     else
         o->fn[PENCIL_POWER] = nullptr;
-    // the h-in-pencil chain: FP32 packed field, 128-point x lines
-    if constexpr (sizeof(T) == sizeof(float) && NX == 128) {
+    // the h-in-pencil chain: FP32 packed field, 96- and 128-point x lines (at 64
+    // the pencil's added h and q traffic cost more than the plane kernel saves)
+    if constexpr (sizeof(T) == sizeof(float) && (NX == 96 || NX == 128)) {
         o->fn[PENCIL_H] = pencil_kernel<T, NX, CW, PENCIL_H>;
         o->fn[PENCIL_H_LAST] = pencil_kernel<T, NX, CW, PENCIL_H_LAST>;
         o->fn[PENCIL_INIT_W] = pencil_kernel<T, NX, CW, PENCIL_INIT_W>;

@@ -3,6 +3,8 @@ restatement; every replica of a mixed-mesh ensemble equals a single
 FP32-mixed context fed the same noise (Anderson counts per step, fields,
 ln Q); a run shaped like the batched configuration (32 replicas, meshes
 32/48/64/96, L = mesh/16, N = 64, NA in [16, 48], XN in [12, 20], C = 50)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -34,7 +36,17 @@ def replicas_small():
 
 
 def single_run(lfts, d, w2, nsteps):
-    s = lfts.System(d["N"], d["NA"], d["XbN"], d["C"], d["dt"], d["m"], d["L"], precision=lfts.LFTS_FP32_MIXED)
+    # the ensemble keeps h in the yz-plane kernel at every mesh; single
+    # contexts at 96^3 and 128^3 default to the h-in-pencil order
+    old = os.environ.get("LFTS_XH_CHAIN")
+    os.environ["LFTS_XH_CHAIN"] = "0"
+    try:
+        s = lfts.System(d["N"], d["NA"], d["XbN"], d["C"], d["dt"], d["m"], d["L"], precision=lfts.LFTS_FP32_MIXED)
+    finally:
+        if old is None:
+            del os.environ["LFTS_XH_CHAIN"]
+        else:
+            os.environ["LFTS_XH_CHAIN"] = old
     M = int(np.prod(d["m"]))
     sigma = float(np.sqrt(2.0 * M * d["dt"] / (d["C"] * np.prod(d["L"]))))
     s.set_fields(w2)
