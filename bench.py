@@ -134,36 +134,113 @@ def make_initial_fields(M, seed):
     return rng.normal(0.0, CFG["init_sd"], 2 * M)
 
 
-# mean Anderson count of this workload (its FP64 path reproduces the
-# reference's iteration counts): the reference arm's steps/s projection
-REFERENCE_K = 31.0
-
-
-def cpu_baseline_sample(K_mean, k_source="the GPU run's mean Anderson K"):
-    """The reference's own calc_concs (oracle/_ref: the reference sources on
-    the FFTW/GSL API shims; else the C oracle port) at the bench configuration,
-    all host threads, projected to steps/s with the GPU run's mean K."""
+def _cpu_objects(threads):
+    """The reference's classes at the bench configuration (oracle/_ref: the
+    reference's own src/*.cc on the FFTW/GSL API shims, `threads` FFT
+    threads), else the C oracle port; (diblock-like object, kind)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
+    m, N, NA = CFG["m"], CFG["N"], CFG["NA"]
+    if pyoracle.RefHarness.available():
+        pyoracle.RefHarness.lib().ref_set_threads(threads)
+        return pyoracle.RefSys(NA, N - NA, m, CFG["L"]), "reference"
+    pyoracle.build_oracle()
+    return pyoracle.Oracle(NA, N - NA, m, CFG["L"], threads=threads), "port"
+
+
+def cpu_baseline_sample(K_mean, k_source):
+    """Bounded CPU sample for the main line: one calc_concs of the reference
+    at the bench configuration on all host threads (~2 s), projected to
+    steps/s with the mean Anderson count K of the reference on this workload
+    (K + 1 calc_concs per step).  The measured complete step is the
+    reference arm's line (--impl reference)."""
     threads = os.cpu_count() or 1
+    M = int(np.prod(CFG["m"]))
+    w = np.zeros(4 * M)
+    w[: 2 * M] = make_initial_fields(M, CFG["field_seed"])
+    obj, kind = _cpu_objects(threads)
+    t0 = time.perf_counter()
+    obj.calc_concs(w)
+    dt = time.perf_counter() - t0
+    obj.close()
+    return {"value": 1.0 / ((K_mean + 1.0) * dt), "unit": "steps/s", "cores": threads, "kind": kind,
+            "sample": f"projection: one calc_concs at 128^3 N=64 ({dt:.2f} s, {threads} threads, the reference's "
+                      f"code on a self-written FFT), steps/s = 1/((K+1) t) with {k_source} = {K_mean:.2f}; "
+                      f"the measured complete step is the --impl reference line",
+            "calc_concs_s": dt}
+
+
+def reference_steps_measured(budget_s=100.0, max_steps=3):
+    """Complete reference Langevin steps at the bench configuration, timed:
+    the reference's own diblock / anderson / langevin objects (oracle/_ref)
+    from the bench's start fields, with its langevin object on
+    mt19937_64(noise seed) as in src/lfts_simulation.cc:23,36; the initial
+    anderson::mix (untimed, src/lfts_simulation.cc:52), then the loop body of
+    src/lfts_simulation.cc:69-76 -- step_wm, mix with the reference's own
+    iteration count, the extra calc_concs -- timed step by step until
+    budget_s is spent (at least one step, at most max_steps)."""
+    threads = os.cpu_count() or 1
+    m, N = CFG["m"], CFG["N"]
+    M = int(np.prod(m))
+    sigma = float(np.sqrt(2.0 * M * CFG["dt"] / (CFG["C"] * np.prod(CFG["L"]))))
+    w = np.zeros(4 * M)
+    w[: 2 * M] = make_initial_fields(M, CFG["field_seed"])
+    obj, kind = _cpu_objects(threads)
+    t0 = time.perf_counter()
+    K0 = obj.mix(w)
+    init_s = time.perf_counter() - t0
+    times, Ks = [], []
+    if kind == "reference":
+        import pyoracle
+        lg = pyoracle.RefLangevin(CFG["noise_seed"], sigma, M)
+        step = lambda: lg.full_step(obj, w, CFG["XN"], CFG["dt"])[0]  # noqa: E731
+    else:
+        # the port (no reference build on this machine): the same loop body,
+        # Gaussian noise of the same sigma from numpy
+        rng = np.random.default_rng(CFG["noise_seed"])
+        prev = [rng.normal(0.0, sigma, M)]
+
+        def step():
+            new = rng.normal(0.0, sigma, M)
+            obj.langevin_update(w, prev[0], new, CFG["XN"], CFG["dt"])
+            prev[0] = new
+            k = obj.mix(w)
+            obj.calc_concs(w)
+            return k
+    while len(times) < max_steps and (not times or sum(times) + times[-1] <= budget_s):
+        t0 = time.perf_counter()
+        Ks.append(int(step()))
+        times.append(time.perf_counter() - t0)
+    obj.close()
+    s = float(np.mean(times))
+    return {"kind": kind, "cores": threads, "s_per_step": s, "K": Ks, "steps_timed": len(times),
+            "init_mix_K": int(K0), "init_mix_s": init_s,
+            "sample": f"{len(times)} complete reference Langevin step(s) at 128^3 N=64 after the initial mix "
+                      f"(step_wm, anderson::mix with its own K = {Ks}, the extra calc_concs), {threads} threads, "
+                      f"the reference's code on a self-written FFT (FFTW is not in the image): {s:.1f} s per step"}
+
+
+def scipy_fft_bound(K_mean, threads=None):
+    """The best CPU FFT in the image (scipy.fft / pocketfft, all host
+    threads) under a restatement of calc_concs (oracle/scipy_path.py): one
+    calc_concs timed, projected to steps/s with K + 1 calc_concs per step.
+    A bound on how much of the GPU/CPU ratio the reference's FFT accounts
+    for -- not the reference."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from scipy_path import ScipyConcs
+    threads = threads or os.cpu_count() or 1
     m, N, NA = CFG["m"], CFG["N"], CFG["NA"]
     M = int(np.prod(m))
     w = np.zeros(4 * M)
     w[: 2 * M] = make_initial_fields(M, CFG["field_seed"])
-    if pyoracle.RefHarness.available():
-        pyoracle.RefHarness.lib().ref_set_threads(threads)
-        obj, kind = pyoracle.RefSys(NA, N - NA, m, CFG["L"]), "reference"
-    else:
-        pyoracle.build_oracle()
-        obj, kind = pyoracle.Oracle(NA, N - NA, m, CFG["L"], threads=threads), "port"
+    sc = ScipyConcs(NA, N - NA, m, CFG["L"], workers=threads)
+    sc.calc_concs(w.copy())  # warm (plans, pages)
     t0 = time.perf_counter()
-    obj.calc_concs(w)
+    sc.calc_concs(w)
     dt = time.perf_counter() - t0
-    steps_per_s = 1.0 / ((K_mean + 1.0) * dt)
-    return {"value": steps_per_s, "unit": "steps/s", "cores": threads, "kind": kind,
-            "sample": f"one calc_concs at 128^3 N=64 ({dt:.2f} s, {threads} threads, shim FFT); "
-                      f"steps/s = 1/((K+1) t) with {k_source} = {K_mean:.2f}",
-            "calc_concs_s": dt}
+    return {"value": 1.0 / ((K_mean + 1.0) * dt), "unit": "steps/s", "cores": threads, "calc_concs_s": dt,
+            "kind": "best available CPU FFT (scipy.fft, pocketfft), not the reference",
+            "sample": f"projection: one calc_concs ({dt:.2f} s) x (K+1) with K = {K_mean:.2f}"}
 
 
 def run_precision(lfts, precision, steps, warmup, rank, device, torch, clocks=None, do_e2e=True):
@@ -296,7 +373,7 @@ def ensemble_bench(lfts, torch, device, steps=5, warmup=3):
            "ms_per_step": ms, "replica_steps_per_s": len(reps) * 1e3 / ms,
            "mean_anderson_K": float(K.mean()),
            "mesh_point_contour_steps_per_s": point_steps * 1e3 / ms,
-           "pencil_cw": {str(d["m"][0]): e.tuning(r) for r, d in enumerate(reps)},
+           "tiles": {str(d["m"][0]): e.tiles(r) for r, d in enumerate(reps)},
            "timing": f"{steps} steps after {warmup} warm-up steps, one CUDA graph launch per step",
            "sequential_single_contexts_ms_per_step": seq_ms,
            "speedup_vs_sequential_single_contexts": seq_ms / ms}
@@ -352,38 +429,95 @@ def max_over_ranks(torch, v, device):
     return v
 
 
-def phi_error_fp32_vs_fp64(lfts, device):
+def _rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def fp32_mixed_errors(lfts, device, nsteps=3):
+    """FP32-mixed against FP64 on the bench workload for each output of the
+    path (phi, H, S(k)):
+      per_call   -- both precisions on the same fields (the FP64 context's
+                    state after the run below): phi (max relative), ln Q and H
+                    (absolute and relative);
+      trajectory -- each precision from the same start with the same noise
+                    (the reference's stream) for nsteps Langevin steps, each
+                    with its own Anderson iterations, S(k) sampled every step:
+                    phi and W- (max relative), H, the binned S(k) (max
+                    difference over bins relative to the largest bin), and
+                    both K sequences."""
     m, N, NA = CFG["m"], CFG["N"], CFG["NA"]
     M = int(np.prod(m))
-    w2 = make_initial_fields(M, 7) * 50.0  # a rougher field than the start
-    out = []
-    for prec in (0, 1):
+    sigma = float(np.sqrt(2.0 * M * CFG["dt"] / (CFG["C"] * np.prod(CFG["L"]))))
+    rng = lfts.Rng(CFG["noise_seed"], sigma)
+    eta = [rng.normal(M) for _ in range(nsteps + 1)]
+    w_start = make_initial_fields(M, CFG["field_seed"])
+    run = {}
+    for prec in (lfts.LFTS_FP64, lfts.LFTS_FP32_MIXED):
         s = lfts.System(N, NA, CFG["XN"], CFG["C"], CFG["dt"], m, CFG["L"], precision=prec, device=device)
-        s.set_fields(w2)
-        lnq = s.calc_concs()
-        out.append((lnq, s.get_fields()[2 * M:]))
-        s.close()
-    err = float(np.max(np.abs(out[1][1] - out[0][1])) / np.max(np.abs(out[0][1])))
-    return err, abs(out[1][0] - out[0][0])
+        s.langevin_init(eta[0])
+        s.set_fields(w_start)
+        s.mix(CFG["max_iter"], CFG["tol"])
+        Ks = []
+        for st in range(1, nsteps + 1):
+            s.langevin_step(eta[st])
+            Ks.append(s.mix(CFG["max_iter"], CFG["tol"]) - 1)
+            s.calc_concs()
+            s.sk_sample()
+        H = s.get_H()
+        _, Sb = s.sk_bin(1e-5)
+        run[prec] = dict(s=s, K=Ks, H=H, w=s.get_fields(), Sb=Sb)
+    a, b = run[lfts.LFTS_FP32_MIXED], run[lfts.LFTS_FP64]
+    traj = {"steps": nsteps, "K_fp64": b["K"], "K_fp32_mixed": a["K"],
+            "phi_rel": _rel(a["w"][2 * M:], b["w"][2 * M:]), "wminus_rel": _rel(a["w"][:M], b["w"][:M]),
+            "H_abs": abs(a["H"] - b["H"]), "H_rel": abs(a["H"] - b["H"]) / abs(b["H"]),
+            "Sk_binned_rel": _rel(a["Sb"], b["Sb"]), "Sk_bins": int(len(b["Sb"]))}
+    s32, s64 = a["s"], b["s"]
+    w2 = b["w"][: 2 * M].copy()
+    s32.set_fields(w2)
+    lnq32 = s32.calc_concs()
+    phi32 = s32.get_fields()[2 * M:]
+    lnq64 = s64.calc_concs()
+    phi64 = s64.get_fields()[2 * M:]
+    H32, H64 = s32.get_H(), s64.get_H()
+    per_call = {"phi_rel": _rel(phi32, phi64), "lnQ_abs": abs(lnq32 - lnq64), "H_abs": abs(H32 - H64),
+                "H_rel": abs(H32 - H64) / abs(H64),
+                "fields": "the FP64 trajectory's state after its last step, given to both precisions"}
+    s32.close()
+    s64.close()
+    return {"per_call": per_call, "trajectory": traj,
+            "note": "S(k) is sampled in FP64 in both precisions, so its error is the W- trajectory's"}
 
 
 def reference_arm(args, rank, world):
+    """The reference's own CPU implementation of the path on this host's
+    cores (oracle/_ref, else the C oracle port): complete Langevin steps at
+    the bench configuration, timed one by one after the initial mix (the
+    warm-up), as many as fit a ~100 s budget (at least one; --steps caps
+    them); plus, labelled, the one-calc_concs projection and its error, and
+    the scipy.fft bound."""
     if rank != 0:
         return 0
-    K_mean = float(os.environ.get("LFTS_BENCH_K", str(REFERENCE_K)))
-    vals = []
-    info = None
-    for i in range(args.warmup + args.steps):
-        info = cpu_baseline_sample(K_mean, "this workload's mean Anderson K (FP64 GPU run, reference counts)")
-        if i >= args.warmup:
-            vals.append(info["value"])
-    v = float(np.mean(vals)) if vals else info["value"]
+    meas = reference_steps_measured(max_steps=max(1, args.steps))
+    v = 1.0 / meas["s_per_step"]
+    iters = float(np.mean(meas["K"])) - 1.0  # anderson::mix returns iterations + 1
+    proj = cpu_baseline_sample(iters, "the measured steps' mean Anderson iteration count")
+    proj_s = 1.0 / proj["value"]
+    extra = {"projection_from_one_calc_concs": {"s_per_step": proj_s, "calc_concs_s": proj["calc_concs_s"],
+                                                "measured_over_projected": meas["s_per_step"] / proj_s}}
+    try:
+        extra["scipy_fft_bound"] = scipy_fft_bound(iters)
+    except Exception as e:  # reported, not fatal
+        extra["scipy_fft_bound"] = {"failed": str(e)}
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(), "cpu_baseline": {k: info[k] for k in ("kind", "cores", "sample")} | {
-                "value": v, "unit": "steps/s"},
+            "steps": meas["steps_timed"], "steps_requested": args.steps,
+            "warmup": f"the initial anderson::mix ({meas['init_mix_K'] - 1} iterations, {meas['init_mix_s']:.1f} s)",
+            "ms_per_step": 1e3 * meas["s_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(),
+            "reference_K": meas["K"], "mean_anderson_K": iters,
+            "cpu_baseline": {"kind": meas["kind"], "cores": meas["cores"], "sample": meas["sample"], "value": v,
+                             "unit": "steps/s"},
             "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    line.update(extra)
     print(json.dumps(line), flush=True)
     return 0
 
@@ -425,10 +559,16 @@ def main(argv=None):
     fp32_sys = fp32.pop("system")
     ms32 = max_over_ranks(torch, fp32["ms_per_step"], device)
     e2e32 = max_over_ranks(torch, fp32["e2e_ms_per_step"], device)
+    # per-step split of the FP32-mixed step: each part of an Anderson
+    # iteration timed on its own (CUDA events, full history), times the
+    # counts per step; the rest is host round trips, launch gaps and the
+    # once-per-step kernels
+    part_chain, part_conc, part_upd = fp32_sys.profile_iteration(5)
     fp32_sys.close()
-    fp64 = run_precision(lfts, lfts.LFTS_FP64, args.steps, args.warmup, rank, device, torch, None, do_e2e=False)
+    fp64 = run_precision(lfts, lfts.LFTS_FP64, args.steps, args.warmup, rank, device, torch, None)
     fp64.pop("system").close()
     ms64 = max_over_ranks(torch, fp64["ms_per_step"], device)
+    e2e64 = max_over_ranks(torch, fp64["e2e_ms_per_step"], device)
 
     if rank == 0:
         m = CFG["m"]
@@ -448,11 +588,21 @@ def main(argv=None):
         W_am_bytes = (3 * 10 + 7) * M * 8
         step_alg = (K_mean + 1) * W_cc_bytes + K_mean * W_am_bytes + 7 * M * 8
         value = world * 1e3 / ms32
-        err_phi, err_lnq = phi_error_fp32_vs_fp64(lfts, device)
+        errs = fp32_mixed_errors(lfts, device)
+        cc_per_step = fp32["calc_concs_per_step"]
+        split = {"chain": cc_per_step * part_chain, "concentrations_and_dots": cc_per_step * part_conc,
+                 "anderson_update": (cc_per_step - 1.0) * part_upd}
+        split["other"] = ms32 - sum(split.values())
+        split_info = {"ms_per_step": split, "ms_per_part": {"chain": part_chain, "concentrations_and_dots": part_conc,
+                                                           "anderson_update": part_upd},
+                      "calc_concs_per_step": cc_per_step,
+                      "other": "host round trips of the Anderson loop, launch gaps, Langevin update"}
+        K64 = float(np.mean(fp64["K"]))
         cpu = None
         if not args.no_cpu_baseline and world == 1:
             try:
-                cpu = cpu_baseline_sample(K_mean)
+                cpu = cpu_baseline_sample(K64, "the FP64 path's mean Anderson iteration count on these steps, "
+                                               "which is the reference's (same start and noise)")
                 cpu.pop("calc_concs_s", None)
             except Exception as e:  # reported, not fatal
                 cpu = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
@@ -489,11 +639,18 @@ def main(argv=None):
             "calc_concs_per_s": fp32["calc_concs_per_step"] * 1e3 / ms32,
             "mesh_point_contour_steps_per_s": fp32["calc_concs_per_step"] * M * (N - 1) * 1e3 / ms32,
             "hbm_gbs_algorithmic_step": step_alg / (ms32 * 1e-3) / 1e9,
-            "fp64": {"value": world * 1e3 / ms64, "ms_per_step": ms64, "mean_anderson_K": float(np.mean(fp64["K"])),
+            "step_split": split_info,
+            "fp64": {"value": world * 1e3 / ms64, "ms_per_step": ms64, "mean_anderson_K": K64,
+                     "e2e": {"value": world * 1e3 / e2e64, "unit": "steps/s",
+                             "h2d_bytes_per_step": fp64["h2d_bytes_per_step"],
+                             "d2h_bytes_per_step": fp64["d2h_bytes_per_step"],
+                             "same_anderson_K": fp64["e2e_same_K"]},
                      "ms_plane": fp64["profile"][0], "ms_pencil": fp64["profile"][1],
                      "calc_concs_per_s": fp64["calc_concs_per_step"] * 1e3 / ms64},
             "speedup_fp32_mixed_vs_fp64": ms64 / ms32,
-            "fp32_phi_rel_err_vs_fp64": err_phi, "fp32_lnQ_abs_err_vs_fp64": err_lnq,
+            "fp32_err_vs_fp64": errs,
+            "fp32_phi_rel_err_vs_fp64": errs["per_call"]["phi_rel"],
+            "fp32_lnQ_abs_err_vs_fp64": errs["per_call"]["lnQ_abs"],
             "ensemble": ens,
         }
         print(json.dumps(line), flush=True)

@@ -30,7 +30,11 @@ typedef enum lfts_status {
     LFTS_ERR_NOMEM = 4,        /* device allocation failed */
     LFTS_ERR_SINGULAR = 5,     /* Anderson least-squares matrix singular */
     LFTS_ERR_STATE = 6,        /* call out of order (e.g. fields never set) */
-    LFTS_ERR_NOTCONV = 7       /* reserved: iteration cap reached where one is fatal */
+    LFTS_ERR_NOTCONV = 7,      /* Anderson mixing stopped at maxIter above the tolerance;
+                                  the fields are updated as the reference leaves them,
+                                  so a caller may carry on (the reference does, silently) */
+    LFTS_ERR_NONFINITE = 8     /* a NaN or infinite Anderson residual: the mix stopped
+                                  before updating w+ with it */
 } lfts_status;
 
 typedef enum lfts_precision {
@@ -78,7 +82,13 @@ int lfts_fields_device(lfts_ctx *ctx, double **w_dev);
 int lfts_calc_concs(lfts_ctx *ctx, double *lnQ);
 
 /* anderson::mix (src/anderson.cc:24-93): saddle point of w+ by Anderson
- * mixing with history 10; *k_out receives the reference's return value. */
+ * mixing with history 10; *k_out receives the reference's return value.
+ * The reference reports no failure; here the loop's end is reported:
+ * LFTS_ERR_NOTCONV when it stopped at maxIter with the error above errTol
+ * (fields and *k_out as the reference leaves them), LFTS_ERR_NONFINITE when
+ * the residual is NaN or infinite (w+ not updated with it; *k_out = the value
+ * the reference's loop returns, which ends there), LFTS_ERR_SINGULAR when the least-squares matrix
+ * is exactly singular (where the reference's GSL solve aborts the program). */
 int lfts_anderson_mix(lfts_ctx *ctx, int maxIter, double errTol, int *k_out);
 
 /* langevin::langevin (src/langevin.cc:7-17): the initial "previous" noise, M
@@ -91,7 +101,9 @@ int lfts_langevin_step(lfts_ctx *ctx, const double *noise_new_host);
 int lfts_langevin_step_device(lfts_ctx *ctx, const double *noise_new_dev);
 
 /* One reference Langevin step (src/lfts_simulation.cc:69-76): step_wm, mix,
- * then the extra calc_concs whose ln Q the reference prints. */
+ * then the extra calc_concs whose ln Q the reference prints.  A mix that ends
+ * with LFTS_ERR_NOTCONV still runs the extra calc_concs (the step completes,
+ * as in the reference) and the call returns LFTS_ERR_NOTCONV. */
 int lfts_langevin_full_step(lfts_ctx *ctx, const double *noise_new_dev, int maxIter,
                             double errTol, int *k_out, double *lnQ);
 
@@ -154,14 +166,38 @@ void *lfts_stream(lfts_ctx *ctx);
  * kernel and of an x-pencil kernel (one stream, events around every launch),
  * and ms of the whole production chain (leaves the current fields' propagators). */
 int lfts_profile_chain(lfts_ctx *ctx, double *ms_plane, double *ms_pencil, double *ms_chain);
+/* Mean ms over `reps` back-to-back runs of each part of one Anderson
+ * iteration on the current fields: the contour chain with Q (one
+ * calc_concs's propagators), the concentration pass with the residual dot
+ * products against a full history (10) and their reduction, and the w+
+ * update over a full history.  A timing helper: the fields, phi and w+ are
+ * left as they were (the update runs with lambda = 0 and zero coefficients). */
+int lfts_profile_iteration(lfts_ctx *ctx, int reps, double *ms_chain, double *ms_concs, double *ms_update);
 /* Number of kernels this context has launched so far. */
 long long lfts_kernel_launches(const lfts_ctx *ctx);
-/* Tile choices of this context's contour chain: x-pencil columns per CTA
- * (picked at lfts_create by timing the chain for 8, 16 and 32 columns, once
- * per precision and mesh in a process; LFTS_AUTOTUNE=0 in the environment
- * keeps the built-in width, LFTS_PENCIL_CW=8|16|32 forces one) and yz-plane
- * transform stages per axis (2; 3 for FP32-mixed 64, 96, 128 square planes).  The tile
- * width does not change results. */
+/* The free choices of a context's contour chain.  None changes what is
+ * computed: pencil_cw changes no value at all, the others change FP32-mixed
+ * results only within that path's stated error (and FP64 ones not at all:
+ * two_streams only reorders independent launches). */
+typedef struct lfts_tiles {
+    int pencil_cw;     /* x-pencil columns per CTA: 8, 16 or 32 */
+    int plane_stages;  /* yz-plane transform stages per axis: 2, or 3 (FP32-mixed, 64/96/128 square planes) */
+    int h_in_pencil;   /* FP32-mixed: h and the propagator stores in the x-pencil kernel and g in the
+                          yz-plane kernel (1; 96- and 128-point x lines, 3 stages), or all in the yz-plane (0) */
+    int two_streams;   /* FP64: each chain on its own stream (1) or both chains in every launch (0) */
+} lfts_tiles;
+/* lfts_create picks the tiles by timing the whole contour chain for every
+ * valid combination on the context's own buffers and keeping the fastest,
+ * once per precision and mesh in a process (the counterpart of the
+ * reference's FFTW_PATIENT planning, src/step.cc:15-16).  Environment:
+ * LFTS_AUTOTUNE=0 skips the timing (built-in choice); LFTS_PENCIL_CW=8|16|32,
+ * LFTS_XH_CHAIN=0|1 and LFTS_ONE_STREAM=1 fix one choice each. */
+int lfts_get_tiles(const lfts_ctx *ctx, lfts_tiles *out);
+/* Installs a tile choice (LFTS_ERR_ARG / LFTS_ERR_UNSUPPORTED for an
+ * invalid one), e.g. to make a context compute exactly what an ensemble
+ * replica with those tiles computes. */
+int lfts_set_tiles(lfts_ctx *ctx, const lfts_tiles *tiles);
+/* pencil_cw and plane_stages of the current tiles */
 int lfts_tuning(const lfts_ctx *ctx, int *pencil_cw, int *plane_stages);
 /* Mean Anderson iteration count of all lfts_anderson_mix calls so far. */
 int lfts_anderson_stats(const lfts_ctx *ctx, long long *calls, long long *iterations);
@@ -204,8 +240,20 @@ int lfts_ensemble_mix(lfts_ensemble *ens, int maxIter, double tol, int *k_out, d
  * lfts_noise_philox(seeds[r], s, M, sigma_r); step 0 is the initial noise,
  * the first call's first step is step 1. */
 int lfts_ensemble_run(lfts_ensemble *ens, int nsteps, int maxIter, double tol, int *k_out, double *lnQ_out);
+/* Mix and run report the most severe status over the replicas and the mixes
+ * of the call (LFTS_ERR_NONFINITE > LFTS_ERR_SINGULAR > LFTS_ERR_NOTCONV, as
+ * for lfts_anderson_mix); a replica that fails stops its own Anderson loop
+ * and leaves the others running.  A run goes on past a mix that stopped at
+ * the cap (the reference does).  This gives replica r's own status of the last
+ * mix or run call. */
+int lfts_ensemble_replica_status(const lfts_ensemble *ens, int r, int *status);
 /* x-pencil columns per CTA of replica r's mesh (autotuned). */
 int lfts_ensemble_tuning(const lfts_ensemble *ens, int r, int *pencil_cw);
+/* The tiles replica r computes with: picked per mesh group by timing the
+ * group's batched contour chain (x-pencil width, yz-plane stages), once per
+ * mesh, group size and N in a process.  A single FP32-mixed context given
+ * these tiles (lfts_set_tiles) computes exactly what the replica computes. */
+int lfts_ensemble_tiles(const lfts_ensemble *ens, int r, lfts_tiles *out);
 /* The CUDA stream the ensemble's graphs run on (a cudaStream_t). */
 void *lfts_ensemble_stream(lfts_ensemble *ens);
 /* Kernels placed in the ensemble's graphs so far (per body iteration). */

@@ -16,9 +16,11 @@ import ctypes as C
 
 import numpy as np
 
-from .capi import LFTS_FP32_MIXED, LFTS_FP64, Input, LftsError, Params, check, lib
+from .capi import (LFTS_ERR_NONFINITE, LFTS_ERR_NOTCONV, LFTS_ERR_SINGULAR, LFTS_FP32_MIXED, LFTS_FP64, LFTS_OK,
+                   Input, LftsError, Params, Tiles, check, check_mix, lib)
 
-__all__ = ["System", "Rng", "read_input", "LftsError", "LFTS_FP64", "LFTS_FP32_MIXED", "lib"]
+__all__ = ["System", "Rng", "read_input", "LftsError", "LFTS_FP64", "LFTS_FP32_MIXED", "LFTS_OK",
+           "LFTS_ERR_SINGULAR", "LFTS_ERR_NOTCONV", "LFTS_ERR_NONFINITE", "lib"]
 
 
 def read_input(path: str) -> Input:
@@ -76,6 +78,8 @@ class Rng:
 class System:
     """One simulated system on one GPU (an lfts_ctx)."""
 
+    last_status = LFTS_OK  # status of the last mix / full step (LFTS_ERR_NOTCONV is not raised)
+
     def __init__(self, N: int, NA: int, XbN: float, C_: float, dt: float, m, L,
                  precision: int = LFTS_FP64, device: int = 0):
         p = Params()
@@ -129,9 +133,13 @@ class System:
         check(lib().lfts_calc_concs(self._h, C.byref(v)), "lfts_calc_concs")
         return v.value
 
-    def mix(self, max_iter: int = 200, tol: float = 1e-4) -> int:
+    def mix(self, max_iter: int = 200, tol: float = 1e-4, strict: bool = False) -> int:
+        """anderson::mix; returns the reference's k.  A loop that stops at
+        max_iter above tol sets ``last_status`` to LFTS_ERR_NOTCONV and raises
+        only with ``strict``; a singular system or a non-finite residual raises."""
         k = C.c_int()
-        check(lib().lfts_anderson_mix(self._h, int(max_iter), float(tol), C.byref(k)), "lfts_anderson_mix")
+        self.last_status = check_mix(lib().lfts_anderson_mix(self._h, int(max_iter), float(tol), C.byref(k)),
+                                     "lfts_anderson_mix", strict)
         return k.value
 
     def langevin_init(self, noise_prev: np.ndarray) -> None:
@@ -145,11 +153,12 @@ class System:
     def langevin_step_device(self, noise_ptr: int) -> None:
         check(lib().lfts_langevin_step_device(self._h, C.c_void_p(noise_ptr)), "lfts_langevin_step_device")
 
-    def full_step_device(self, noise_ptr: int, max_iter: int = 200, tol: float = 1e-4):
+    def full_step_device(self, noise_ptr: int, max_iter: int = 200, tol: float = 1e-4, strict: bool = False):
         k = C.c_int()
         lnq = C.c_double()
-        check(lib().lfts_langevin_full_step(self._h, C.c_void_p(noise_ptr), int(max_iter), float(tol),
-                                            C.byref(k), C.byref(lnq)), "lfts_langevin_full_step")
+        self.last_status = check_mix(lib().lfts_langevin_full_step(self._h, C.c_void_p(noise_ptr), int(max_iter),
+                                                                   float(tol), C.byref(k), C.byref(lnq)),
+                                     "lfts_langevin_full_step", strict)
         return k.value, lnq.value
 
     def sk_sample(self) -> None:
@@ -215,10 +224,28 @@ class System:
         check(lib().lfts_tuning(self._h, C.byref(a), C.byref(b)), "lfts_tuning")
         return a.value, b.value
 
+    def tiles(self) -> dict:
+        """the contour chain's tile choice (lfts_tiles) as a dict"""
+        t = Tiles()
+        check(lib().lfts_get_tiles(self._h, C.byref(t)), "lfts_get_tiles")
+        return t.as_dict()
+
+    def set_tiles(self, pencil_cw: int, plane_stages: int, h_in_pencil: int = 0, two_streams: int = 0) -> None:
+        t = Tiles(int(pencil_cw), int(plane_stages), int(h_in_pencil), int(two_streams))
+        check(lib().lfts_set_tiles(self._h, C.byref(t)), "lfts_set_tiles")
+
     def profile_chain(self):
         """(ms per yz-plane step kernel, ms per x-pencil kernel, ms per chain)"""
         a, b, c = C.c_double(), C.c_double(), C.c_double()
         check(lib().lfts_profile_chain(self._h, C.byref(a), C.byref(b), C.byref(c)), "lfts_profile_chain")
+        return a.value, b.value, c.value
+
+    def profile_iteration(self, reps: int = 5):
+        """(ms chain, ms concentrations + dot products, ms w+ update) of one
+        Anderson iteration with a full history; fields unchanged"""
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        check(lib().lfts_profile_iteration(self._h, int(reps), C.byref(a), C.byref(b), C.byref(c)),
+              "lfts_profile_iteration")
         return a.value, b.value, c.value
 
     def anderson_stats(self):
@@ -244,6 +271,8 @@ class Ensemble:
     """Independent FP32-mixed replicas advanced together (an lfts_ensemble).
 
     replicas: list of dicts with keys N, NA, XbN, C, dt, m, L and seed."""
+
+    last_status = LFTS_OK  # most severe replica status of the last mix / run
 
     def __init__(self, replicas, device: int = 0):
         n = len(replicas)
@@ -288,26 +317,41 @@ class Ensemble:
         check(lib().lfts_ensemble_get_fields(self._h, int(r), out), "lfts_ensemble_get_fields")
         return out
 
-    def mix(self, max_iter: int = 200, tol: float = 1e-4):
-        """(K per replica, ln Q per replica)"""
+    def mix(self, max_iter: int = 200, tol: float = 1e-4, strict: bool = False):
+        """(K per replica, ln Q per replica); statuses as System.mix, per
+        replica in replica_status()"""
         k = np.zeros(self.nrep, dtype=np.int32)
         lnq = np.zeros(self.nrep)
-        check(lib().lfts_ensemble_mix(self._h, int(max_iter), float(tol), k.ctypes.data, lnq.ctypes.data),
-              "lfts_ensemble_mix")
+        self.last_status = check_mix(lib().lfts_ensemble_mix(self._h, int(max_iter), float(tol), k.ctypes.data,
+                                                             lnq.ctypes.data), "lfts_ensemble_mix", strict)
         return k, lnq
 
-    def run(self, nsteps: int, max_iter: int = 200, tol: float = 1e-4, record_k: bool = True):
+    def run(self, nsteps: int, max_iter: int = 200, tol: float = 1e-4, record_k: bool = True,
+            strict: bool = False):
         """(K[nsteps][nrep] or None, ln Q per replica after the last step)"""
         k = np.zeros((nsteps, self.nrep), dtype=np.int32) if record_k else None
         lnq = np.zeros(self.nrep)
-        check(lib().lfts_ensemble_run(self._h, int(nsteps), int(max_iter), float(tol),
-                                      k.ctypes.data if record_k else None, lnq.ctypes.data), "lfts_ensemble_run")
+        self.last_status = check_mix(lib().lfts_ensemble_run(self._h, int(nsteps), int(max_iter), float(tol),
+                                                             k.ctypes.data if record_k else None, lnq.ctypes.data),
+                                     "lfts_ensemble_run", strict)
         return k, lnq
+
+    def replica_status(self, r: int) -> int:
+        """lfts_status of replica r's last mix or run"""
+        s = C.c_int()
+        check(lib().lfts_ensemble_replica_status(self._h, int(r), C.byref(s)), "lfts_ensemble_replica_status")
+        return s.value
 
     def tuning(self, r: int) -> int:
         cw = C.c_int()
         check(lib().lfts_ensemble_tuning(self._h, int(r), C.byref(cw)), "lfts_ensemble_tuning")
         return cw.value
+
+    def tiles(self, r: int) -> dict:
+        """replica r's tile choice (batched autotuning), as System.tiles()"""
+        t = Tiles()
+        check(lib().lfts_ensemble_tiles(self._h, int(r), C.byref(t)), "lfts_ensemble_tiles")
+        return t.as_dict()
 
     def stream(self) -> int:
         return int(lib().lfts_ensemble_stream(self._h) or 0)

@@ -17,6 +17,12 @@ LIB_PATH = os.path.join(PKG, "liblfts_b200.so")
 LFTS_FP64 = 0
 LFTS_FP32_MIXED = 1
 
+# lfts_status codes that callers act on
+LFTS_OK = 0
+LFTS_ERR_SINGULAR = 5
+LFTS_ERR_NOTCONV = 7
+LFTS_ERR_NONFINITE = 8
+
 
 class LftsError(RuntimeError):
     def __init__(self, status: int, what: str):
@@ -39,6 +45,14 @@ class Input(C.Structure):
                 ("sample_freq", C.c_int), ("save_freq", C.c_int), ("loadType", C.c_int),
                 ("XbN", C.c_double), ("XeN", C.c_double), ("V", C.c_double), ("sigma", C.c_double),
                 ("M", C.c_longlong), ("Mk", C.c_longlong)]
+
+
+class Tiles(C.Structure):
+    _fields_ = [("pencil_cw", C.c_int), ("plane_stages", C.c_int), ("h_in_pencil", C.c_int),
+                ("two_streams", C.c_int)]
+
+    def as_dict(self):
+        return {f: int(getattr(self, f)) for f, _ in self._fields_}
 
 
 _lib = None
@@ -77,7 +91,12 @@ SIGNATURES = {
     "lfts_stream": (C.c_void_p, [_P]),
     "lfts_kernel_launches": (C.c_longlong, [_P]),
     "lfts_tuning": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "lfts_get_tiles": (C.c_int, [_P, C.POINTER(Tiles)]),
+    "lfts_set_tiles": (C.c_int, [_P, C.POINTER(Tiles)]),
+    "lfts_ensemble_tiles": (C.c_int, [_P, C.c_int, C.POINTER(Tiles)]),
     "lfts_profile_chain": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "lfts_profile_iteration": (C.c_int, [_P, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                         C.POINTER(C.c_double)]),
     "lfts_anderson_stats": (C.c_int, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "lfts_get_propagators": (C.c_int, [_P, _dp]),
     "lfts_ensemble_create": (C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
@@ -86,6 +105,7 @@ SIGNATURES = {
     "lfts_ensemble_get_fields": (C.c_int, [_P, C.c_int, _dp]),
     "lfts_ensemble_mix": (C.c_int, [_P, C.c_int, C.c_double, C.c_void_p, C.c_void_p]),
     "lfts_ensemble_run": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p]),
+    "lfts_ensemble_replica_status": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
     "lfts_ensemble_tuning": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
     "lfts_ensemble_stream": (C.c_void_p, [_P]),
     "lfts_ensemble_kernel_launches": (C.c_longlong, [_P]),
@@ -122,3 +142,13 @@ def lib():
 def check(status: int, what: str) -> None:
     if status != 0:
         raise LftsError(status, what)
+
+
+def check_mix(status: int, what: str, strict: bool) -> int:
+    """As check(), except that an Anderson mix stopped at its iteration cap
+    (LFTS_ERR_NOTCONV) is returned rather than raised unless ``strict``: the
+    reference carries on past the cap, and so do callers that mirror it."""
+    if status == LFTS_ERR_NOTCONV and not strict:
+        return status
+    check(status, what)
+    return status

@@ -38,6 +38,8 @@ struct EnsRep {
     int cur;              // physical buffer of the current iteration
     int k;                // iteration number (src/anderson.cc:31)
     int active, stopped, done, go, simple, singular;
+    int notconv, nonfinite;  // loop ended at maxIter above tol; NaN or infinite residual
+    int sticky;              // OR over the mixes of one host call: 1 notconv, 2 singular, 4 nonfinite
     int iters;            // k at loop exit (the value anderson::mix returns)
     double coef[kMaxHist];
     double DD[kRedWidth][kRedWidth];
@@ -272,7 +274,17 @@ __global__ void __launch_bounds__(256) ens_reduce_solve_kernel(EnsRep *__restric
     __syncwarp();
     if (lane == 0) {
         R.simple = k < 2;
-        if (!ok) {
+        // err = (S1/M)^(1/2) (the reference takes pow(., 0.5); sqrt is the
+        // correctly rounded value of the same)
+        const double err = sqrt(__ddiv_rn(DD00, (double)R.M));
+        if (!isfinite(err)) {
+            // a NaN or infinite residual: stop before w+ is updated with it
+            // (the reference would update and then leave the loop, as NaN > tol
+            // is false)
+            R.nonfinite = 1;
+            R.stopped = 1;
+            R.go = 0;
+        } else if (!ok) {
             R.singular = 1;
             R.stopped = 1;
             R.go = 0;
@@ -283,10 +295,10 @@ __global__ void __launch_bounds__(256) ens_reduce_solve_kernel(EnsRep *__restric
             R.DD[n][n] = DD00;
             for (int c = 1; c < n; c++) R.DD[c][n] = dd0[c];
             for (int c = n + 1; c <= nh; c++) R.DD[n][c] = dd0[c];
-            // err = (S1/M)^(1/2) (the reference takes pow(., 0.5); sqrt is the
-            // correctly rounded value of the same)
-            const double err = sqrt(__ddiv_rn(DD00, (double)R.M));
-            if (!(err > tol) || !(k + 1 < maxIter)) R.stopped = 1;
+            if (!(err > tol) || !(k + 1 < maxIter)) {
+                R.stopped = 1;
+                R.notconv = err > tol;  // the loop ends at the cap, above the tolerance
+            }
         }
     }
 }
@@ -321,6 +333,7 @@ __global__ void ens_control_kernel(EnsRep *__restrict__ reps, int nrep, cudaGrap
         if (R.done) {
             R.active = 0;
             R.iters = R.k;
+            R.sticky |= (R.notconv ? 1 : 0) | (R.singular ? 2 : 0) | (R.nonfinite ? 4 : 0);
             continue;
         }
         if (R.go) {
@@ -344,9 +357,15 @@ __global__ void ens_begin_kernel(EnsRep *__restrict__ reps, int nrep, long long 
         EnsRep &R = reps[r];
         R.k = 1;
         R.active = 1;
-        R.stopped = R.done = R.go = R.singular = 0;
+        R.stopped = R.done = R.go = R.singular = R.notconv = R.nonfinite = 0;
     }
     if (advance && threadIdx.x == 0) *step += 1;
+}
+
+// clears the replicas' status bits at the start of a host call (mix or run)
+__global__ void ens_clear_status_kernel(EnsRep *__restrict__ reps, int nrep)
+{
+    for (int r = threadIdx.x; r < nrep; r += blockDim.x) reps[r].sticky = 0;
 }
 
 // W- += -(phi- + 2 W-/XbN) dt + (eta_prev + eta_new)/2 (src/langevin.cc:31),

@@ -387,6 +387,14 @@ void enqueue_concs(lfts_ctx *c, void *Dh0, int nh, const HistPtrs &hist)
     }
 }
 
+void enqueue_chain_any(lfts_ctx *c)
+{
+    if (c->prec == LFTS_FP64)
+        enqueue_chain<double>(c);
+    else
+        enqueue_chain<float>(c);
+}
+
 void enqueue_concs_any(lfts_ctx *c, void *Dh0, int nh, const HistPtrs &hist)
 {
     if (c->prec == LFTS_FP64)
@@ -395,13 +403,24 @@ void enqueue_concs_any(lfts_ctx *c, void *Dh0, int nh, const HistPtrs &hist)
         enqueue_concs<float>(c, Dh0, nh, hist);
 }
 
-// ---- x-pencil tile width ------------------------------------------------------
-// Picked by timing the whole contour chain (the pencil's cost depends on how
-// its tiles overlap the neighbouring plane kernels, so it is timed in place)
-// for each candidate width on the context's own buffers, once per precision
-// and mesh per process.  Column arithmetic does not depend on the width.
+// ---- tile choices and their autotuner ------------------------------------------
+// A context's contour chain has these free choices, none of which changes what
+// is computed (each is tested against the others at the precision's tolerance;
+// the x-pencil width changes no column's arithmetic at all):
+//   pencil_cw     x-pencil columns per CTA (8, 16, 32)
+//   plane_stages  FP32-mixed yz-plane transform stages per axis: 3 (fft_plane3.cuh,
+//                 64 / 96 / 128 square planes) or 2 (fft_packed.cuh)
+//   h_in_pencil   FP32-mixed: h and the propagator stores in the x-pencil and g in
+//                 the yz-plane kernel (96- and 128-point x lines, three-stage planes),
+//                 or both in the yz-plane kernel
+//   two_streams   FP64: each chain on its own stream, or both chains per launch
+// autotune() times the whole chain for every valid combination on the
+// context's own buffers (a tile's cost depends on how it overlaps its
+// neighbours in the chain, so it is timed in place) and keeps the fastest,
+// once per (precision, mesh) per process -- the reference's analogue is
+// planning its FFTs with FFTW_PATIENT (src/step.cc:15-16).
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int>, int> g_tuned_cw;
+std::map<std::tuple<int, int, int, int>, lfts_tiles> g_tuned;
 
 template <typename T>
 int set_pencil(lfts_ctx *c, int cw)
@@ -414,58 +433,161 @@ int set_pencil(lfts_ctx *c, int cw)
     return LFTS_OK;
 }
 
-template <typename T>
-int tune_pencil(lfts_ctx *c, int *best_cw)
+void drop_chain_graph(lfts_ctx *c)
 {
-    static const int cands[] = {8, 16, 32};
+    if (c->chain_exec) cudaGraphExecDestroy(c->chain_exec);
+    if (c->chain_graph) cudaGraphDestroy(c->chain_graph);
+    c->chain_exec = nullptr;
+    c->chain_graph = nullptr;
+}
+
+// installs a tile choice (validated); the chain graph is captured anew
+int apply_tiles(lfts_ctx *c, const lfts_tiles &t)
+{
+    if (t.pencil_cw != 8 && t.pencil_cw != 16 && t.pencil_cw != 32) return LFTS_ERR_ARG;
+    if (c->prec == LFTS_FP64) {
+        if (t.plane_stages != 2 || t.h_in_pencil != 0 || (t.two_streams != 0 && t.two_streams != 1))
+            return LFTS_ERR_ARG;
+        int rc = set_pencil<double>(c, t.pencil_cw);
+        if (rc) return rc;
+        c->two_streams = t.two_streams == 1;
+    } else {
+        if ((t.plane_stages != 2 && t.plane_stages != 3) || (t.h_in_pencil != 0 && t.h_in_pencil != 1) ||
+            t.two_streams != 0)
+            return LFTS_ERR_ARG;
+        PlaneKernels<float> pl{};
+        const bool ok = t.plane_stages == 3 ? plane3_kernels(c->my, c->mz, &pl) : plane_c_kernels(c->my, c->mz, &pl);
+        if (!ok) return LFTS_ERR_UNSUPPORTED;
+        PencilKernels<float> pk{};
+        if (!pencil_kernels(c->mx, t.pencil_cw, &pk)) return LFTS_ERR_UNSUPPORTED;
+        if (t.h_in_pencil && !(pl.fn[PLANE_G] && pk.fn[PENCIL_H])) return LFTS_ERR_UNSUPPORTED;
+        for (int m = 0; m < kPlaneModes; m++)
+            if (pl.fn[m]) CK(cudaFuncSetAttribute(pl.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
+        int rc = set_pencil<float>(c, t.pencil_cw);
+        if (rc) return rc;
+        c->pl32 = pl;
+        c->plane_stages = t.plane_stages;
+        c->xh_chain = t.h_in_pencil == 1;
+    }
+    drop_chain_graph(c);
+    return LFTS_OK;
+}
+
+lfts_tiles current_tiles(const lfts_ctx *c)
+{
+    lfts_tiles t{};
+    const bool fp64 = c->prec == LFTS_FP64;
+    t.pencil_cw = fp64 ? c->pe64.cw : c->pe32.cw;
+    t.plane_stages = fp64 ? 2 : c->plane_stages;
+    t.h_in_pencil = (!fp64 && c->xh_chain) ? 1 : 0;
+    t.two_streams = (fp64 && c->two_streams) ? 1 : 0;
+    return t;
+}
+
+// every valid combination for this context, restricted by the environment
+// (LFTS_PENCIL_CW, LFTS_XH_CHAIN, LFTS_ONE_STREAM fix one choice each)
+std::vector<lfts_tiles> tile_candidates(const lfts_ctx *c)
+{
+    std::vector<lfts_tiles> out;
+    const char *fcw = std::getenv("LFTS_PENCIL_CW");
+    const char *fxh = std::getenv("LFTS_XH_CHAIN");
+    const char *fone = std::getenv("LFTS_ONE_STREAM");
+    const int cw_forced = fcw ? std::atoi(fcw) : 0;
+    for (int cw : {8, 16, 32}) {
+        if (cw_forced > 0 && cw != cw_forced) continue;
+        if (c->prec == LFTS_FP64) {
+            for (int two : {1, 0}) {
+                if (fone && ((fone[0] == '1') == (two == 1))) continue;
+                out.push_back({cw, 2, 0, two});
+            }
+            continue;
+        }
+        PlaneKernels<float> p3{};
+        PencilKernels<float> pk{};
+        const bool has3 = plane3_kernels(c->my, c->mz, &p3);
+        const bool hasx = has3 && p3.fn[PLANE_G] && pencil_kernels(c->mx, cw, &pk) && pk.fn[PENCIL_H];
+        for (int st : {3, 2}) {
+            if (st == 3 && !has3) continue;
+            for (int xh : {1, 0}) {
+                if (xh && (st != 3 || !hasx)) continue;
+                if (fxh && ((fxh[0] != '0') != (xh == 1))) continue;
+                out.push_back({cw, st, xh, 0});
+            }
+        }
+    }
+    return out;
+}
+
+// the choice used when autotuning is off: three-stage planes and h in the
+// x-pencil where compiled, the usual pencil winners, two FP64 streams
+lfts_tiles default_tiles(const lfts_ctx *c)
+{
+    std::vector<lfts_tiles> cand = tile_candidates(c);
+    const int cw = c->prec == LFTS_FP64 ? kDefaultCwFp64 : kDefaultCwFp32;
+    for (const lfts_tiles &t : cand)
+        if (t.pencil_cw == cw) return t;  // candidates come best-guess first
+    return cand.empty() ? lfts_tiles{cw, 2, 0, c->prec == LFTS_FP64 ? 1 : 0} : cand.front();
+}
+
+template <typename T>
+int time_chain(lfts_ctx *c, cudaEvent_t e0, cudaEvent_t e1, float *ms)
+{
+    enqueue_chain_launches<T>(c);  // warm-up
+    CK(cudaEventRecord(e0, c->st));
+    for (int r = 0; r < 3; r++) enqueue_chain_launches<T>(c);
+    CK(cudaEventRecord(e1, c->st));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaGetLastError());
+    CK(cudaEventElapsedTime(ms, e0, e1));
+    return LFTS_OK;
+}
+
+int tune_tiles(lfts_ctx *c, lfts_tiles *best)
+{
     const long long launches0 = c->launches;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    float best = 0.f;
-    *best_cw = 0;
-    for (int cw : cands) {
-        if (set_pencil<T>(c, cw) != LFTS_OK) continue;
-        enqueue_chain_launches<T>(c);  // warm-up
-        CK(cudaEventRecord(e0, c->st));
-        for (int r = 0; r < 3; r++) enqueue_chain_launches<T>(c);
-        CK(cudaEventRecord(e1, c->st));
-        CK(cudaEventSynchronize(e1));
+    float best_ms = 0.f;
+    bool found = false;
+    int rc = LFTS_OK;
+    for (const lfts_tiles &t : tile_candidates(c)) {
+        if (apply_tiles(c, t) != LFTS_OK) continue;
         float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, e0, e1));
-        if (*best_cw == 0 || ms < best) {
-            best = ms;
-            *best_cw = cw;
+        rc = c->prec == LFTS_FP64 ? time_chain<double>(c, e0, e1, &ms) : time_chain<float>(c, e0, e1, &ms);
+        if (rc) break;
+        if (!found || ms < best_ms) {
+            best_ms = ms;
+            *best = t;
+            found = true;
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    CK(cudaStreamSynchronize(c->st));
     c->launches = launches0;
-    return *best_cw ? LFTS_OK : LFTS_ERR_UNSUPPORTED;
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaStreamSynchronize(c->st1));
+    return found ? LFTS_OK : LFTS_ERR_UNSUPPORTED;
 }
 
 int autotune(lfts_ctx *c)
 {
-    const bool fp64 = c->prec == LFTS_FP64;
-    int cw = fp64 ? kDefaultCwFp64 : kDefaultCwFp32;
+    lfts_tiles t = default_tiles(c);
     const char *e = std::getenv("LFTS_AUTOTUNE");
-    const char *forced = std::getenv("LFTS_PENCIL_CW");
-    if (forced && std::atoi(forced) > 0) {
-        cw = std::atoi(forced);
-    } else if (!(e && e[0] == '0')) {
+    if (!(e && e[0] == '0')) {
         const auto key = std::make_tuple(c->prec, c->mx, c->my, c->mz);
         std::lock_guard<std::mutex> lk(g_tune_mu);
-        auto it = g_tuned_cw.find(key);
-        if (it != g_tuned_cw.end()) {
-            cw = it->second;
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) {
+            t = it->second;
         } else {
-            int rc = fp64 ? tune_pencil<double>(c, &cw) : tune_pencil<float>(c, &cw);
+            int rc = tune_tiles(c, &t);
             if (rc) return rc;
-            g_tuned_cw[key] = cw;
+            g_tuned[key] = t;
         }
     }
-    return fp64 ? set_pencil<double>(c, cw) : set_pencil<float>(c, cw);
+    return apply_tiles(c, t);
 }
 
 // One chain on one stream with CUDA events around every contour-step kernel
@@ -591,6 +713,14 @@ int anderson_mix(lfts_ctx *c, int maxIter, double errTol, int *k_out)
         CK(cudaStreamSynchronize(c->st));
         const double S1 = c->red_host[0];
         err = std::pow(S1 / (double)M, 0.5);
+        if (!std::isfinite(err)) {
+            // stop before w+ is updated with it; k_out is what the reference's
+            // loop would return (NaN > tol ends it after this iteration)
+            g_last_error = "NaN or infinite Anderson residual (non-finite fields or concentrations)";
+            c->mix_calls++;
+            if (k_out) *k_out = k + 1;
+            return LFTS_ERR_NONFINITE;
+        }
         const double lambda = 1.0 - std::pow(0.9, double(k));
         for (int m = 0; m <= nh; m++) c->DD[0][m] = c->red_host[m];
 
@@ -636,6 +766,10 @@ int anderson_mix(lfts_ctx *c, int maxIter, double errTol, int *k_out)
     c->mix_calls++;
     if (k_out) *k_out = k;
     c->have_concs = true;
+    if (err > errTol) {  // the loop ended at maxIter
+        g_last_error = "Anderson mixing stopped at maxIter with the error above the tolerance";
+        return LFTS_ERR_NOTCONV;
+    }
     return LFTS_OK;
 }
 
@@ -951,7 +1085,8 @@ const char *lfts_status_string(int s)
         case LFTS_ERR_NOMEM: return "device allocation failed";
         case LFTS_ERR_SINGULAR: return "Anderson least-squares matrix singular";
         case LFTS_ERR_STATE: return "call out of order";
-        case LFTS_ERR_NOTCONV: return "iteration cap reached";
+        case LFTS_ERR_NOTCONV: return "Anderson iteration cap reached above the tolerance";
+        case LFTS_ERR_NONFINITE: return "non-finite Anderson residual";
         default: return "unknown status";
     }
 }
@@ -1157,9 +1292,11 @@ int lfts_langevin_full_step(lfts_ctx *c, const double *noise_new_dev, int maxIte
     if (!c->fields_set || !c->eta_set || !c->have_concs) return LFTS_ERR_STATE;
     DeviceGuard g(c->dev);
     int rc = langevin_device(c, noise_new_dev);
-    if (!rc) rc = anderson_mix(c, maxIter, errTol, k_out);
-    if (!rc) rc = calc_concs_sync(c, lnQ);
-    return rc;
+    if (rc) return rc;
+    rc = anderson_mix(c, maxIter, errTol, k_out);
+    if (rc && rc != LFTS_ERR_NOTCONV) return rc;
+    const int rc2 = calc_concs_sync(c, lnQ);  // the step completes past the cap, as in the reference
+    return rc2 ? rc2 : rc;
 }
 
 int lfts_sk_sample(lfts_ctx *c)
@@ -1351,6 +1488,83 @@ int lfts_profile_chain(lfts_ctx *c, double *ms_plane, double *ms_pencil, double 
     CK(cudaStreamSynchronize(c->st));
     if (c->prec == LFTS_FP64) return profile_chain<double>(c, ms_plane, ms_pencil, ms_chain);
     return profile_chain<float>(c, ms_plane, ms_pencil, ms_chain);
+}
+
+int lfts_profile_iteration(lfts_ctx *c, int reps, double *ms_chain, double *ms_concs, double *ms_update)
+{
+    if (!c || reps < 1 || !ms_chain || !ms_concs || !ms_update) return LFTS_ERR_ARG;
+    if (!c->fields_set) return LFTS_ERR_STATE;
+    DeviceGuard g(c->dev);
+    CK(cudaStreamSynchronize(c->st));
+    const long long M = c->M;
+    // a full history: every ring buffer in use, as from the 11th iteration on
+    HistPtrs Dhp{}, whp{};
+    for (int m = 1; m <= kMaxHist; m++) {
+        Dhp.p[m - 1] = c->Dh[c->phys[m]];
+        whp.p[m - 1] = c->wh[c->phys[m]];
+    }
+    Coefs zero{};  // lambda = 0 and zero coefficients leave w+ bitwise unchanged
+    cudaEvent_t ev[4];
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    enqueue_chain_any(c);  // warm
+    CK(cudaEventRecord(ev[0], c->st));
+    for (int r = 0; r < reps; r++) enqueue_chain_any(c);
+    CK(cudaEventRecord(ev[1], c->st));
+    for (int r = 0; r < reps; r++) {
+        if (c->prec == LFTS_FP64)
+            concentrations_kernel<double><<<stream_grid(c), kRedThreads, 0, c->st>>>(
+                static_cast<const double *>(c->q), M, c->N, c->NA, c->w, c->w + 2 * M, c->w + 3 * M, c->Qd,
+                static_cast<double *>(c->Dh[c->cur]), kMaxHist, Dhp, c->partials);
+        else
+            concentrations_kernel<float><<<stream_grid(c), kRedThreads, 0, c->st>>>(
+                static_cast<const float *>(c->q), M, c->N, c->NA, c->w, c->w + 2 * M, c->w + 3 * M, c->Qd,
+                static_cast<float *>(c->Dh[c->cur]), kMaxHist, Dhp, c->partials);
+        reduce_partials_kernel<<<1, 256, 0, c->st>>>(c->partials, c->red_blocks, kRedWidth, c->red);
+    }
+    CK(cudaEventRecord(ev[2], c->st));
+    for (int r = 0; r < reps; r++) {
+        if (c->prec == LFTS_FP64)
+            anderson_update_kernel<double><<<stream_grid(c), 256, 0, c->st>>>(
+                c->w + M, static_cast<double *>(c->wh[c->cur]), static_cast<const double *>(c->Dh[c->cur]), M, 0.0,
+                kMaxHist, 0, Dhp, whp, zero);
+        else
+            anderson_update_kernel<float><<<stream_grid(c), 256, 0, c->st>>>(
+                c->w + M, static_cast<float *>(c->wh[c->cur]), static_cast<const float *>(c->Dh[c->cur]), M, 0.0,
+                kMaxHist, 0, Dhp, whp, zero);
+    }
+    CK(cudaEventRecord(ev[3], c->st));
+    CK(cudaEventSynchronize(ev[3]));
+    CK(cudaGetLastError());
+    float t[3];
+    for (int i = 0; i < 3; i++) CK(cudaEventElapsedTime(&t[i], ev[i], ev[i + 1]));
+    for (auto &e : ev) cudaEventDestroy(e);
+    c->launches += (long long)reps * 3;
+    *ms_chain = t[0] / reps;
+    *ms_concs = t[1] / reps;
+    *ms_update = t[2] / reps;
+    return LFTS_OK;
+}
+
+int lfts_get_tiles(const lfts_ctx *c, lfts_tiles *out)
+{
+    if (!c || !out) return LFTS_ERR_ARG;
+    *out = current_tiles(c);
+    return LFTS_OK;
+}
+
+int lfts_set_tiles(lfts_ctx *c, const lfts_tiles *t)
+{
+    if (!c || !t) return LFTS_ERR_ARG;
+    DeviceGuard g(c->dev);
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaStreamSynchronize(c->st1));
+    const lfts_tiles old = current_tiles(c);
+    int rc = apply_tiles(c, *t);
+    if (rc) {
+        apply_tiles(c, old);  // leave the context as it was
+        g_last_error = "tile choice not valid for this context's precision and mesh";
+    }
+    return rc;
 }
 
 int lfts_tuning(const lfts_ctx *c, int *pencil_cw, int *plane_stages)

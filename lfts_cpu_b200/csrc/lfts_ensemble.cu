@@ -12,8 +12,12 @@
 //
 // so a step costs one graph launch and no host round trip.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -86,19 +90,24 @@ void fill_plane3(PlaneSet *o)
     o->smem = C3::SMEM;
 }
 
-// the plane kernel a single FP32 context of this mesh uses (plane3_kernels /
-// plane_c_kernels), so that replicas reproduce single contexts
-bool ens_plane(int ny, int nz, PlaneSet *o)
+// yz-plane kernels of an ensemble mesh: three transform stages per axis
+// (fft_plane3.cuh: 64 and 96 planes) or two (fft_packed.cuh), the same bodies
+// a single FP32-mixed context runs with those tiles
+bool ens_plane(int ny, int nz, int stages, PlaneSet *o)
 {
     if (ny != nz) return false;
-    if (ny == 96) {
-        fill_plane3<Plane3_96>(o);
-        return true;
+    if (stages == 3) {
+        if (ny == 96) {
+            fill_plane3<Plane3_96>(o);
+            return true;
+        }
+        if (ny == 64) {
+            fill_plane3<Plane3_64>(o);
+            return true;
+        }
+        return false;
     }
-    if (ny == 64) {
-        fill_plane3<Plane3_64>(o);
-        return true;
-    }
+    if (stages != 2) return false;
 #define X(n)                    \
     if (ny == n) {              \
         fill_plane<n>(o);       \
@@ -124,7 +133,7 @@ bool ens_pencil(int nx, int cw, PencilSet *o)
 }
 
 struct Group {
-    int mx = 0, my = 0, mz = 0, cw = 0;
+    int mx = 0, my = 0, mz = 0, cw = 0, stages = 2;
     std::vector<int> members;
     int *d_members = nullptr;
     PlaneSet pl{};
@@ -153,6 +162,7 @@ struct lfts_ensemble {
     int g_maxIter = -1;
     double g_tol = -1.0;
     long long launches = 0;
+    std::vector<int> status;  // each replica's status after the last mix / run
 };
 
 namespace {
@@ -302,21 +312,135 @@ int ensure_graphs(lfts_ensemble *e, int maxIter, double tol)
     return LFTS_OK;
 }
 
+// ---- batched tile choice ---------------------------------------------------------
+// Each mesh group's tiles (x-pencil width 8/16/32; yz-plane stages 3 or 2 where
+// both exist) are picked by timing the group's batched contour chain, all its
+// replicas active, on its own stream -- batched, the best tiles differ from a
+// single context's (the plane launches run in several waves) -- once per
+// (mesh, group size, N) per process.  The choice is installed in every member
+// context too, so lfts_get_tiles on a replica's context, or lfts_set_tiles on
+// a single context, gives exactly the tiles the replica computes with.
+std::mutex g_ens_tune_mu;
+std::map<std::tuple<int, int, int, int, int>, std::pair<int, int>> g_ens_tuned;  // -> (cw, stages)
+
+int set_group_tiles(Group &g, int cw, int stages)
+{
+    PlaneSet pl{};
+    PencilSet pe{};
+    if (!ens_plane(g.my, g.mz, stages, &pl) || !ens_pencil(g.mx, cw, &pe)) return LFTS_ERR_UNSUPPORTED;
+    for (int m = 0; m < 4; m++)
+        EK(cudaFuncSetAttribute(pl.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
+    EK(cudaFuncSetAttribute(pe.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pe.smem));
+    g.pl = pl;
+    g.pe = pe;
+    g.cw = cw;
+    g.stages = stages;
+    return LFTS_OK;
+}
+
+void enqueue_group_chain(lfts_ensemble *e, Group &g)
+{
+    const int nm = (int)g.members.size();
+    const dim3 pgrid(g.mx, nm);
+    const dim3 egrid((g.my * g.mz + g.cw - 1) / g.cw, nm);
+    g.pl.fn[PLANE_INIT_W]<<<pgrid, g.pl.nt, g.pl.smem, g.st>>>(e->d_reps, g.d_members, 0);
+    for (int i = 1; i < e->N; i++) {
+        g.pe.fn<<<egrid, g.pe.nt, g.pe.smem, g.st>>>(e->d_reps, g.d_members);
+        g.pl.fn[i + 1 < e->N ? PLANE_STEP : PLANE_LAST]<<<pgrid, g.pl.nt, g.pl.smem, g.st>>>(e->d_reps, g.d_members,
+                                                                                           i);
+    }
+}
+
+int tune_groups(lfts_ensemble *e)
+{
+    const char *off = std::getenv("LFTS_AUTOTUNE");
+    const char *fcw = std::getenv("LFTS_PENCIL_CW");
+    const int cw_forced = fcw ? std::atoi(fcw) : 0;
+    // every replica active, so that the batched kernels do their work
+    ens_begin_kernel<<<1, 256, 0, e->s0>>>(e->d_reps, e->nrep, e->d_step, 0);
+    EK(cudaStreamSynchronize(e->s0));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    EK(cudaEventCreate(&e0));
+    EK(cudaEventCreate(&e1));
+    int rc = LFTS_OK;
+    for (Group &g : e->groups) {
+        const auto key = std::make_tuple(g.mx, g.my, g.mz, (int)g.members.size(), e->N);
+        std::pair<int, int> best{cw_forced > 0 ? cw_forced : 16, 2};
+        PlaneSet p3{};
+        if (ens_plane(g.my, g.mz, 3, &p3)) best.second = 3;
+        if (!(off && off[0] == '0')) {
+            std::lock_guard<std::mutex> lk(g_ens_tune_mu);
+            auto it = g_ens_tuned.find(key);
+            if (it != g_ens_tuned.end()) {
+                best = it->second;
+            } else {
+                float best_ms = 0.f;
+                bool found = false;
+                for (int stages : {3, 2})
+                    for (int cw : {8, 16, 32}) {
+                        if (cw_forced > 0 && cw != cw_forced) continue;
+                        if (set_group_tiles(g, cw, stages) != LFTS_OK) continue;
+                        enqueue_group_chain(e, g);  // warm-up
+                        cudaEventRecord(e0, g.st);
+                        for (int r = 0; r < 3; r++) enqueue_group_chain(e, g);
+                        cudaEventRecord(e1, g.st);
+                        cudaError_t ce = cudaEventSynchronize(e1);
+                        if (ce == cudaSuccess) ce = cudaGetLastError();
+                        float ms = 0.f;
+                        if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+                        if (ce != cudaSuccess) {
+                            lfts_internal_set_error(cudaGetErrorString(ce));
+                            rc = LFTS_ERR_CUDA;
+                            break;
+                        }
+                        if (!found || ms < best_ms) {
+                            best_ms = ms;
+                            best = {cw, stages};
+                            found = true;
+                        }
+                    }
+                if (rc) break;
+                if (found) g_ens_tuned[key] = best;
+            }
+        }
+        if ((rc = set_group_tiles(g, best.first, best.second))) break;
+        const lfts_tiles t{best.first, best.second, 0, 0};
+        for (int r : g.members)
+            if ((rc = lfts_set_tiles(e->rep[r], &t))) break;
+        if (rc) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+
 int read_back(lfts_ensemble *e, int *k_out, double *lnQ_out)
 {
     EK(cudaStreamSynchronize(e->s0));
     EK(cudaMemcpy(e->h_reps.data(), e->d_reps, sizeof(EnsRep) * e->nrep, cudaMemcpyDeviceToHost));
-    int singular = -1;
+    // the most severe replica status: non-finite residual, singular system,
+    // iteration cap (each replica's own status: lfts_ensemble_replica_status)
+    int worst = LFTS_OK, worst_r = -1;
+    auto rank = [](int s) { return s == LFTS_ERR_NONFINITE ? 3 : s == LFTS_ERR_SINGULAR ? 2 : s ? 1 : 0; };
     for (int r = 0; r < e->nrep; r++) {
-        if (k_out) k_out[r] = e->h_reps[r].iters;
-        if (e->h_reps[r].singular && singular < 0) singular = r;
-        if (lnQ_out) EK(cudaMemcpy(&lnQ_out[r], e->h_reps[r].Qd + 1, sizeof(double), cudaMemcpyDeviceToHost));
+        const EnsRep &R = e->h_reps[r];
+        if (k_out) k_out[r] = R.iters;
+        const int s = (R.sticky & 4) ? LFTS_ERR_NONFINITE : (R.sticky & 2) ? LFTS_ERR_SINGULAR
+                                                          : (R.sticky & 1) ? LFTS_ERR_NOTCONV : LFTS_OK;
+        e->status[r] = s;
+        if (rank(s) > rank(worst)) {
+            worst = s;
+            worst_r = r;
+        }
+        if (lnQ_out) EK(cudaMemcpy(&lnQ_out[r], R.Qd + 1, sizeof(double), cudaMemcpyDeviceToHost));
     }
-    if (singular >= 0) {
-        lfts_internal_set_error("Anderson least-squares matrix is singular in a replica");
-        return LFTS_ERR_SINGULAR;
+    if (worst != LFTS_OK) {
+        const char *what = worst == LFTS_ERR_NONFINITE ? "a NaN or infinite Anderson residual"
+                           : worst == LFTS_ERR_SINGULAR ? "a singular Anderson least-squares matrix"
+                                                        : "Anderson mixing stopped at maxIter above the tolerance";
+        lfts_internal_set_error((std::string(what) + " in replica " + std::to_string(worst_r)).c_str());
     }
-    return LFTS_OK;
+    return worst;
 }
 
 }  // namespace
@@ -336,7 +460,7 @@ int lfts_ensemble_create(const lfts_params *params, const unsigned long long *se
         }
         PlaneSet ps;
         PencilSet qs;
-        if (!ens_plane(p.m[1], p.m[2], &ps) || !ens_pencil(p.m[0], 16, &qs)) {
+        if (!ens_plane(p.m[1], p.m[2], 2, &ps) || !ens_pencil(p.m[0], 16, &qs)) {
             lfts_internal_set_error("ensemble meshes: 16, 24, 32, 48, 64 or 96 points per side, cubic planes");
             return LFTS_ERR_UNSUPPORTED;
         }
@@ -357,6 +481,7 @@ int lfts_ensemble_create(const lfts_params *params, const unsigned long long *se
         e->rep.push_back(c);
     }
     e->h_reps.resize(nrep);
+    e->status.assign(nrep, LFTS_OK);
     for (int r = 0; r < nrep; r++) {
         lfts_ctx *c = e->rep[r];
         EnsRep &R = e->h_reps[r];
@@ -401,8 +526,9 @@ int lfts_ensemble_create(const lfts_params *params, const unsigned long long *se
             g.mx = c->mx;
             g.my = c->my;
             g.mz = c->mz;
-            g.cw = c->pe32.cw;
-            ens_plane(g.my, g.mz, &g.pl);
+            g.cw = 16;
+            g.stages = 2;
+            ens_plane(g.my, g.mz, g.stages, &g.pl);
             if (!ens_pencil(g.mx, g.cw, &g.pe)) return fail(LFTS_ERR_UNSUPPORTED);
             e->groups.push_back(g);
             gi = (int)e->groups.size() - 1;
@@ -433,6 +559,8 @@ int lfts_ensemble_create(const lfts_params *params, const unsigned long long *se
         cudaMalloc(&e->d_step, sizeof(long long)) != cudaSuccess ||
         cudaMemcpy(e->d_step, &step1, sizeof(long long), cudaMemcpyHostToDevice) != cudaSuccess)
         return fail(LFTS_ERR_NOMEM);
+    int rc = tune_groups(e);
+    if (rc) return fail(rc);
     *out = e;
     return LFTS_OK;
 }
@@ -480,6 +608,7 @@ int lfts_ensemble_mix(lfts_ensemble *e, int maxIter, double tol, int *k_out, dou
     EnsDeviceGuard dg(e->dev);
     int rc = ensure_graphs(e, maxIter, tol);
     if (rc) return rc;
+    ens_clear_status_kernel<<<1, 256, 0, e->s0>>>(e->d_reps, e->nrep);
     EK(cudaGraphLaunch(e->x_mix, e->s0));
     return read_back(e, k_out, lnQ_out);
 }
@@ -490,14 +619,24 @@ int lfts_ensemble_run(lfts_ensemble *e, int nsteps, int maxIter, double tol, int
     EnsDeviceGuard dg(e->dev);
     int rc = ensure_graphs(e, maxIter, tol);
     if (rc) return rc;
+    ens_clear_status_kernel<<<1, 256, 0, e->s0>>>(e->d_reps, e->nrep);
     for (int s = 0; s < nsteps; s++) {
         EK(cudaGraphLaunch(e->x_step, e->s0));
         if (k_out) {
+            // a mix that stopped at the cap completes its step and the run goes
+            // on (the reference's loop does); any other failure ends the run
             rc = read_back(e, k_out + (long long)s * e->nrep, nullptr);
-            if (rc) return rc;
+            if (rc && rc != LFTS_ERR_NOTCONV) return rc;
         }
     }
     return read_back(e, nullptr, lnQ_out);
+}
+
+int lfts_ensemble_replica_status(const lfts_ensemble *e, int r, int *status)
+{
+    if (!e || r < 0 || r >= e->nrep || !status) return LFTS_ERR_ARG;
+    *status = e->status[r];
+    return LFTS_OK;
 }
 
 int lfts_ensemble_tuning(const lfts_ensemble *e, int r, int *pencil_cw)
@@ -505,6 +644,12 @@ int lfts_ensemble_tuning(const lfts_ensemble *e, int r, int *pencil_cw)
     if (!e || r < 0 || r >= e->nrep) return LFTS_ERR_ARG;
     if (pencil_cw) *pencil_cw = e->rep[r]->pe32.cw;
     return LFTS_OK;
+}
+
+int lfts_ensemble_tiles(const lfts_ensemble *e, int r, lfts_tiles *out)
+{
+    if (!e || r < 0 || r >= e->nrep || !out) return LFTS_ERR_ARG;
+    return lfts_get_tiles(e->rep[r], out);
 }
 
 void *lfts_ensemble_stream(lfts_ensemble *e) { return e ? (void *)e->s0 : nullptr; }

@@ -21,6 +21,7 @@
 //    that device current); make that first call before any stream capture.
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 #include <string>
 
 #include <cuda_runtime.h>
@@ -50,7 +51,14 @@ struct NoallocLayout {
 static __device__ __align__(256) unsigned char g_step_scratch[NoallocLayout::bytes];
 
 constexpr int kMaxDevices = 64;
-unsigned char *g_scratch_addr[kMaxDevices] = {};  // device address of g_step_scratch per device
+// device address of g_step_scratch per device, looked up once per device
+// (std::call_once: host threads making their first calls together wait for
+// one lookup).  The address belongs to the device's primary context: after
+// cudaDeviceReset on a device it is stale, like every other handle of this
+// library on that device.
+unsigned char *g_scratch_addr[kMaxDevices] = {};
+std::once_flag g_scratch_once[kMaxDevices];
+cudaError_t g_scratch_err[kMaxDevices] = {};
 
 // twiddles exp(-2 pi i t/n) and the factorised Boltzmann weight of
 // src/step.cc:69-89 (1/M folded into the z factor), computed on the device
@@ -88,12 +96,13 @@ int fail(int code, const char *msg)
 // dynamic shared-memory limits of the kernels this mesh uses.
 int device_setup(int dev, const PlaneKernels<double> &pl, const PencilKernels<double> &pe)
 {
-    if (!g_scratch_addr[dev]) {
+    std::call_once(g_scratch_once[dev], [dev] {
         void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_step_scratch);
-        if (e != cudaSuccess || !p) return fail(LFTS_ERR_CUDA, "cudaGetSymbolAddress(g_step_scratch) failed");
-        g_scratch_addr[dev] = static_cast<unsigned char *>(p);
-    }
+        g_scratch_err[dev] = cudaGetSymbolAddress(&p, g_step_scratch);
+        if (g_scratch_err[dev] == cudaSuccess && p) g_scratch_addr[dev] = static_cast<unsigned char *>(p);
+    });
+    if (g_scratch_err[dev] != cudaSuccess || !g_scratch_addr[dev])
+        return fail(LFTS_ERR_CUDA, "cudaGetSymbolAddress(g_step_scratch) failed");
     for (int m = 0; m < 4; m++)
         if (cudaFuncSetAttribute(pl.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem) != cudaSuccess)
             return fail(LFTS_ERR_CUDA, "cudaFuncSetAttribute failed");
@@ -116,6 +125,9 @@ int lfts_step_fwd_noalloc(const lfts_params *p, const double *q_in, double *q_ou
         return fail(LFTS_ERR_ARG, "chain lengths or monomer index out of range");
     if (mx < 1 || my < 1 || mz < 1 || mx > kMaxLen || my > kMaxLen || mz > kMaxLen)
         return fail(LFTS_ERR_ARG, "mesh dimension above the no-alloc limit of 128");
+    for (int d = 0; d < 3; d++)
+        if (!(p->L[d] > 0.0) || !std::isfinite(p->L[d]))
+            return fail(LFTS_ERR_ARG, "box lengths must be positive and finite");
     const long long KZ = mz / 2 + 1;
     if (2LL * mx * my * KZ > kMaxSpec)
         return fail(LFTS_ERR_ARG, "mesh above the no-alloc scratch limit: 2*mx*my*(mz/2+1) must be <= "

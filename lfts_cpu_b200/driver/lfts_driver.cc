@@ -23,6 +23,13 @@ namespace {
 
 void die_on(int status, const char *what)
 {
+    if (status == LFTS_ERR_NOTCONV) {
+        // the reference carries on silently when anderson::mix reaches its
+        // cap; the run goes on here too, with a note on stderr (stdout and the
+        // output files stay the reference program's)
+        std::cerr << "lfts-b200: " << what << ": " << lfts_status_string(status) << " (continuing)" << std::endl;
+        return;
+    }
     if (status != LFTS_OK) {
         std::cerr << "lfts-b200: " << what << ": " << lfts_status_string(status);
         const char *e = lfts_last_error_string();

@@ -219,6 +219,12 @@ class RefHarness:
             lib.ref_sim_sk_save.argtypes = [C.c_void_p, C.c_char_p]
             lib.ref_sim_sk_raw.argtypes = [C.c_void_p, _dp, C.POINTER(C.c_int)]
             lib.ref_normal_stream.argtypes = [C.c_ulonglong, C.c_double, C.c_int, _dp]
+            lib.ref_lamellar.argtypes = [_dp, C.c_double, C.c_void_p]
+            lib.ref_lgv_create.restype = C.c_void_p
+            lib.ref_lgv_create.argtypes = [C.c_ulonglong, C.c_double, C.c_int]
+            lib.ref_lgv_destroy.argtypes = [C.c_void_p]
+            lib.ref_sys_full_step.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double, _dp,
+                                              C.POINTER(C.c_int), C.POINTER(C.c_double)]
             cls._lib = lib
         return cls._lib
 
@@ -255,6 +261,39 @@ class RefSys:
         out = np.empty(self.Mk)
         self._lib.ref_sys_g(self._s, out, self.Mk)
         return out
+
+
+def ref_lamellar(amp, m):
+    """W-, w+ (2M) of the reference's (300) lamellar start, amplitude amp."""
+    M = int(m[0]) * int(m[1]) * int(m[2])
+    w = np.zeros(2 * M)
+    RefHarness.lib().ref_lamellar(w, float(amp), _i3(m))
+    return w
+
+
+class RefLangevin:
+    """The reference's langevin object on its own mt19937_64(seed); its
+    constructor draws the initial noise.  ``full_step`` runs the reference's
+    loop body (step_wm, mix, the extra calc_concs) on a RefSys."""
+
+    def __init__(self, seed, sigma, M):
+        self._lib = RefHarness.lib()
+        self.sigma = float(sigma)
+        self._l = self._lib.ref_lgv_create(int(seed), self.sigma, int(M))
+
+    def close(self):
+        if self._l:
+            self._lib.ref_lgv_destroy(self._l)
+            self._l = None
+
+    __del__ = close
+
+    def full_step(self, sys_: RefSys, w, XbN, dt):
+        K = C.c_int()
+        lnQ = C.c_double()
+        self._lib.ref_sys_full_step(sys_._s, self._l, float(XbN), self.sigma, float(dt), w, C.byref(K),
+                                    C.byref(lnQ))
+        return K.value, lnQ.value
 
 
 class RefSim:

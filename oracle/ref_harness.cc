@@ -84,6 +84,33 @@ void ref_sys_step_fwd(ref_sys *s, const double *q_in, double *q_out, const doubl
 
 void ref_sys_g(ref_sys *s, double *g, int Mk) { std::memcpy(g, s->stp->g_.get(), sizeof(double) * Mk); }
 
+/* The reference's langevin object (src/langevin.cc:7-17) on its own
+ * mt19937_64 seeded with `seed`: the constructor draws the initial "previous"
+ * noise.  One Langevin step below is the loop body of
+ * src/lfts_simulation.cc:69-76: step_wm, mix (200, 1e-4), the extra calc_concs. */
+struct ref_lgv {
+    std::mt19937_64 rng;
+    std::unique_ptr<langevin> lgv;
+};
+
+ref_lgv *ref_lgv_create(unsigned long long seed, double sigma, int M)
+{
+    ref_lgv *l = new ref_lgv;
+    l->rng.seed(seed);
+    l->lgv = std::make_unique<langevin>(l->rng, sigma, M);
+    return l;
+}
+
+void ref_lgv_destroy(ref_lgv *l) { delete l; }
+
+void ref_sys_full_step(ref_sys *s, ref_lgv *l, double XbN, double sigma, double dt, double *w, int *K,
+                       double *lnQ)
+{
+    l->lgv->step_wm(w, l->rng, XbN, sigma, dt);
+    *K = s->am->mix(s->dbc.get(), 200, 1e-4, w);
+    *lnQ = s->dbc->calc_concs(w);
+}
+
 void ref_set_threads(int n)
 {
     fftw_init_threads();
@@ -162,6 +189,14 @@ void ref_sim_sk_raw(ref_sim *r, double *S, int *nsamples)
 
 void ref_sim_equilibrate(ref_sim *r) { r->sim->equilibrate(); }
 void ref_sim_statistics(ref_sim *r) { r->sim->statistics(); }
+
+/* field_generator::create_lamellar (src/field_generator.h:11-24): the (300)
+ * lamellar W- of amplitude amp, w+ = 0, into w[0, 2M) */
+void ref_lamellar(double *w, double amp, const int *m_in)
+{
+    int m[3] = {m_in[0], m_in[1], m_in[2]};
+    field_generator::create_lamellar(w, amp, m);
+}
 
 /* draws from a fresh mt19937_64(seed) + normal_distribution(0, sigma) */
 void ref_normal_stream(unsigned long long seed, double sigma, int n, double *out)

@@ -6,7 +6,9 @@ stores inputs and outputs at full precision.  Needs the reference tree (build
 with ``make -C oracle all``); the fixtures it writes are committed, so the
 tests never need the reference at run time.
 
-    python tests/golden/make_golden.py
+    LFTS_REFERENCE=<reference tree> python tests/golden/make_golden.py [case ...]
+
+With case names, only those fixtures are written (see CASES below).
 """
 from __future__ import annotations
 
@@ -24,7 +26,7 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 from pyoracle import RefHarness, RefSim, RefSys, build_oracle  # noqa: E402
 
-REF_TREE = os.environ.get("LFTS_REFERENCE", "/root/reference")
+REF_TREE = os.environ.get("LFTS_REFERENCE")
 
 
 def write_input(path, hdr, fields=None):
@@ -105,6 +107,82 @@ def case_trajectory(name, hdr, n_eq, n_st, sample_every=1, fields=None):
         shutil.rmtree(work, ignore_errors=True)
 
 
+def _compact(prefix, w, M, stride):
+    """A 4M field array as every stride-th value plus per-quarter sums and sums of squares."""
+    q = w.reshape(4, M)
+    return {prefix + "_s": w[::stride].copy(), prefix + "_sum": q.sum(axis=1), prefix + "_sq": (q * q).sum(axis=1)}
+
+
+def case_config(name, hdr, n_steps, stride, field_seed=None, sample_every=1, sensitivity=False):
+    """A run at one of the benchmark configurations' own sizes (N = 64), kept
+    compact: 4M field arrays are stored as every stride-th value plus
+    per-quarter sums.  Stores
+      * calc_concs of the start fields (RefSys): ln Q, phi;
+      * with ``sensitivity``: whether the reference's own mix of the start
+        fields changes its iteration count under a 1e-15 relative perturbation;
+      * the reference constructor's initial mix (RefSim): the mixed fields;
+      * n_steps Langevin steps: K and ln Q per step, S(k) samples, fields, H.
+    Start fields: a seeded Gaussian (numpy default_rng(field_seed), mean 0,
+    sd 0.01, fed as loadType 1) or the reference's own generator (loadType 2)."""
+    (N, NA, XN, C, dt, isXeN), (m, L), rest = hdr
+    M = int(np.prod(m))
+    out = {"stride": stride}
+    fields = None
+    if field_seed is not None:
+        fields = np.random.default_rng(field_seed).normal(0.0, 0.01, 2 * M)
+        out.update(field_seed=field_seed, fields_sum=fields.reshape(2, M).sum(axis=1))
+        start = fields.copy()
+    else:
+        from pyoracle import ref_lamellar
+        start = ref_lamellar(XN, m)  # isXeN = 0: XbN = XN
+    sys_ = RefSys(NA, N - NA, m, L)
+    w = np.zeros(4 * M)
+    w[:2 * M] = start
+    out["cc_lnQ"] = sys_.calc_concs(w)
+    out.update(_compact("cc_w", w, M, stride))
+    if sensitivity:
+        ks = []
+        for eps in (0.0, 1e-15):
+            wp = np.zeros(4 * M)
+            wp[:2 * M] = start * (1.0 + eps)
+            ks.append(sys_.mix(wp))
+            sys_.close()
+            sys_ = RefSys(NA, N - NA, m, L)
+        out["mix_K_unperturbed"], out["mix_K_perturbed"] = ks
+        print(name, "mix K with and without a 1e-15 perturbation", ks)
+    sys_.close()
+    work = tempfile.mkdtemp()
+    cwd = os.getcwd()
+    try:
+        os.chdir(work)
+        write_input("input", hdr, fields)
+        sim = RefSim("input")
+        out.update(_compact("w0", sim.w(), M, stride))
+        Ks, lnQs = [], []
+        for it in range(1, n_steps + 1):
+            k, l = sim.step(sample=(it % sample_every == 0))
+            Ks.append(k)
+            lnQs.append(l)
+        out.update(_compact("w_end", sim.w(), M, stride))
+        S, ns = sim.sk_raw()
+        sim.sk_save("struct_out")
+        with open("struct_out") as f:
+            out["struct_text"] = f.read()
+        out["H"] = sim.getH()
+        out.update(_compact("w_H", sim.w(), M, stride))  # phi of getH's calc_concs: of the final fields
+        out.update(header=np.array([open("input").read().split("\n")[i] for i in range(3)]), N=sim.N, NA=sim.NA,
+                   m=np.array(sim.m), L=np.array(L), XbN=sim.XbN, sigma=sim.sigma, CV=sim.CV, dt=sim.dt,
+                   loadType=sim.loadType, K=np.array(Ks), lnQ=np.array(lnQs), S_s=S[::stride], S_sum=S.sum(),
+                   nsamples=ns, n_steps=n_steps,
+                   sample_every=sample_every)
+        sim.close()
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        print(name, "K", Ks, "H", out["H"], "M", M)
+    finally:
+        os.chdir(cwd)
+        shutil.rmtree(work, ignore_errors=True)
+
+
 def case_ref_input40(name):
     """calc_concs and one mix on the reference's own 40^3 fixture field
     (input_files/input, loadType 1)."""
@@ -152,30 +230,64 @@ def case_program_run(name, hdr):
         shutil.rmtree(work, ignore_errors=True)
 
 
-def main():
+CASES = {
+    "comp_16": lambda: case_components("comp_16", 6, 10, (16, 16, 16), (3.2, 3.0, 3.4), 11, 2.0, 0.5),
+    "comp_12x24x16": lambda: case_components("comp_12x24x16", 7, 9, (12, 24, 16), (2.5, 4.1, 3.3), 12, 1.5, 0.3,
+                                             steps=(2, 8, 15)),
+    "comp_8x12x20": lambda: case_components("comp_8x12x20", 3, 5, (8, 12, 20), (2.0, 2.4, 3.0), 13, 1.0, 0.2,
+                                            steps=(1, 4, 7)),
+    # the reference CI's valgrind input (tests/valgrind/input_valgrind): 16^3, N=90, random start
+    "traj_valgrind16": lambda: case_trajectory(
+        "traj_valgrind16", ((90, 40, 13.15, 100.0, 1.0, 1), ((16, 16, 16), (4.38, 4.38, 4.38)), (1, 1, 1, 1000, 3)),
+        1, 1),
+    # a small disordered-start run with S(k) sampling
+    "traj_16": lambda: case_trajectory(
+        "traj_16", ((16, 6, 12.0, 50.0, 0.5, 0), ((16, 16, 16), (3.0, 3.0, 3.0)), (3, 4, 1, 1000, 0)), 3, 4,
+        sample_every=1),
+    # lamellar (300) start at 24^3
+    "traj_lam24": lambda: case_trajectory(
+        "traj_lam24", ((24, 12, 16.0, 100.0, 0.5, 0), ((24, 24, 24), (3.6, 3.6, 3.6)), (2, 2, 1, 1000, 2)), 2, 2,
+        sample_every=1),
+    "ref_input40": lambda: case_ref_input40("ref_input40"),
+    # the reference CI's valgrind input, run by the reference program itself
+    "prog_valgrind16": lambda: case_program_run(
+        "prog_valgrind16", ((90, 40, 13.15, 100.0, 1.0, 1), ((16, 16, 16), (4.38, 4.38, 4.38)), (1, 1, 1, 1000, 3))),
+    # a disordered-start run that saves and samples every step
+    "prog_saves16": lambda: case_program_run(
+        "prog_saves16", ((16, 6, 12.0, 50.0, 0.5, 0), ((16, 16, 16), (3.0, 3.0, 3.0)), (2, 2, 1, 1, 0))),
+    # plain-FP64 configuration, CPU-runnable: 32^3, N=64, NA=32, XN=14, C=50,
+    # dt=0.5, L=4, seeded Gaussian (sd 0.01) start; initial mix + 10 steps,
+    # S(k) sampled every step
+    "cfg1_32": lambda: case_config(
+        "cfg1_32", ((64, 32, 14.0, 50.0, 0.5, 0), ((32, 32, 32), (4.0, 4.0, 4.0)), (1000, 1000, 10, 1000000, 1)),
+        10, 7, field_seed=101, sample_every=1, sensitivity=True),
+    # plain-FP64 B200 configuration: 64^3, N=64, NA=32, XN=16, C=100, dt=0.5,
+    # L=6.4, (300) lamellar start; initial mix + 3 steps
+    "cfg2_64": lambda: case_config(
+        "cfg2_64", ((64, 32, 16.0, 100.0, 0.5, 0), ((64, 64, 64), (6.4, 6.4, 6.4)), (5000, 5000, 20, 1000000, 2)),
+        3, 61, sample_every=1, sensitivity=True),
+    # adjoint configuration: 64^3, N=64, NA=32, XN=15, C=50, L=6.0, lamellar;
+    # the mixed start (phi) and H after one step
+    "cfg4_64": lambda: case_config(
+        "cfg4_64", ((64, 32, 15.0, 50.0, 0.5, 0), ((64, 64, 64), (6.0, 6.0, 6.0)), (10, 10, 1, 1000000, 2)),
+        1, 61, sample_every=1, sensitivity=True),
+}
+
+
+def main(argv=None):
+    names = list(argv if argv is not None else sys.argv[1:]) or list(CASES)
+    unknown = [n for n in names if n not in CASES]
+    if unknown:
+        raise SystemExit(f"unknown cases {unknown}; known: {sorted(CASES)}")
+    if not REF_TREE or not os.path.isdir(os.path.join(REF_TREE, "src")):
+        raise SystemExit("LFTS_REFERENCE must name the reference project's tree")
+    os.environ["REF"] = REF_TREE
     build_oracle(ref=True)
     if not RefHarness.available():
         raise SystemExit("oracle/_ref/libref_harness.so missing: the reference tree is needed")
     RefHarness.lib().ref_quiet(1)
-    case_components("comp_16", 6, 10, (16, 16, 16), (3.2, 3.0, 3.4), 11, 2.0, 0.5)
-    case_components("comp_12x24x16", 7, 9, (12, 24, 16), (2.5, 4.1, 3.3), 12, 1.5, 0.3, steps=(2, 8, 15))
-    case_components("comp_8x12x20", 3, 5, (8, 12, 20), (2.0, 2.4, 3.0), 13, 1.0, 0.2, steps=(1, 4, 7))
-    # the reference CI's valgrind input (tests/valgrind/input_valgrind): 16^3, N=90, random start
-    case_trajectory("traj_valgrind16", ((90, 40, 13.15, 100.0, 1.0, 1), ((16, 16, 16), (4.38, 4.38, 4.38)),
-                                        (1, 1, 1, 1000, 3)), 1, 1)
-    # a small disordered-start run with S(k) sampling
-    case_trajectory("traj_16", ((16, 6, 12.0, 50.0, 0.5, 0), ((16, 16, 16), (3.0, 3.0, 3.0)),
-                                (3, 4, 1, 1000, 0)), 3, 4, sample_every=1)
-    # lamellar (300) start at 24^3
-    case_trajectory("traj_lam24", ((24, 12, 16.0, 100.0, 0.5, 0), ((24, 24, 24), (3.6, 3.6, 3.6)),
-                                   (2, 2, 1, 1000, 2)), 2, 2, sample_every=1)
-    case_ref_input40("ref_input40")
-    # the reference CI's valgrind input, run by the reference program itself
-    case_program_run("prog_valgrind16", ((90, 40, 13.15, 100.0, 1.0, 1), ((16, 16, 16), (4.38, 4.38, 4.38)),
-                                         (1, 1, 1, 1000, 3)))
-    # a disordered-start run that saves and samples every step
-    case_program_run("prog_saves16", ((16, 6, 12.0, 50.0, 0.5, 0), ((16, 16, 16), (3.0, 3.0, 3.0)),
-                                      (2, 2, 1, 1, 0)))
+    for n in names:
+        CASES[n]()
 
 
 if __name__ == "__main__":

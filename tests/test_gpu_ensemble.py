@@ -3,8 +3,6 @@ restatement; every replica of a mixed-mesh ensemble equals a single
 FP32-mixed context fed the same noise (Anderson counts per step, fields,
 ln Q); a run shaped like the batched configuration (32 replicas, meshes
 32/48/64/96, L = mesh/16, N = 64, NA in [16, 48], XN in [12, 20], C = 50)."""
-import os
-
 import numpy as np
 import pytest
 
@@ -35,18 +33,13 @@ def replicas_small():
     ]
 
 
-def single_run(lfts, d, w2, nsteps):
-    # the ensemble keeps h in the yz-plane kernel at every mesh; single
-    # contexts at 96^3 and 128^3 default to the h-in-pencil order
-    old = os.environ.get("LFTS_XH_CHAIN")
-    os.environ["LFTS_XH_CHAIN"] = "0"
-    try:
-        s = lfts.System(d["N"], d["NA"], d["XbN"], d["C"], d["dt"], d["m"], d["L"], precision=lfts.LFTS_FP32_MIXED)
-    finally:
-        if old is None:
-            del os.environ["LFTS_XH_CHAIN"]
-        else:
-            os.environ["LFTS_XH_CHAIN"] = old
+def single_run(lfts, d, w2, nsteps, tiles):
+    # a single FP32-mixed context with the replica's tiles (the ensemble picks
+    # its tiles by timing its batched chain; they can differ from the tiles a
+    # lone context of the same mesh picks)
+    s = lfts.System(d["N"], d["NA"], d["XbN"], d["C"], d["dt"], d["m"], d["L"], precision=lfts.LFTS_FP32_MIXED)
+    s.set_tiles(**tiles)
+    assert s.tiles() == tiles
     M = int(np.prod(d["m"]))
     sigma = float(np.sqrt(2.0 * M * d["dt"] / (d["C"] * np.prod(d["L"]))))
     s.set_fields(w2)
@@ -76,9 +69,10 @@ def test_replicas_equal_single_contexts(lfts):
     nsteps = 3
     ks, lnq = e.run(nsteps)
     w = [e.get_fields(r) for r in range(len(reps))]
+    tiles = [e.tiles(r) for r in range(len(reps))]
     e.close()
     for r, d in enumerate(reps):
-        sk0, slnq0, sw0, sks, slnq, sw = single_run(lfts, d, fields[r], nsteps)
+        sk0, slnq0, sw0, sks, slnq, sw = single_run(lfts, d, fields[r], nsteps, tiles[r])
         assert k0[r] == sk0
         assert lnq0[r] == slnq0
         assert np.array_equal(w0[r], sw0)
@@ -104,6 +98,10 @@ def test_batched_configuration_shape(lfts):
     k0, _ = e.mix()
     ks, lnq = e.run(2)
     assert all(e.tuning(r) in (8, 16, 32) for r in range(32))
+    for r, mm in enumerate(meshes):
+        t = e.tiles(r)
+        assert t["h_in_pencil"] == 0 and t["two_streams"] == 0
+        assert t["plane_stages"] in ((3, 2) if mm in (64, 96) else (2,))
     for r, d in enumerate(reps):
         w = e.get_fields(r)
         M = int(np.prod(d["m"]))
@@ -115,7 +113,7 @@ def test_batched_configuration_shape(lfts):
         if mm in checked:
             continue
         checked.add(mm)
-        sk0, _, _, sks, slnq, sw = single_run(lfts, reps[r], fields[r], 2)
+        sk0, _, _, sks, slnq, sw = single_run(lfts, reps[r], fields[r], 2, e.tiles(r))
         assert k0[r] == sk0 and list(ks[:, r]) == sks
         assert lnq[r] == slnq
         assert np.array_equal(e.get_fields(r), sw)

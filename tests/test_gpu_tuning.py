@@ -1,11 +1,18 @@
-"""Autotuned tile shapes of the contour chain: the x-pencil tile width is
-bitwise-neutral, and the autotuner's choice is one of the candidates."""
-import os
+"""Tile choices of the contour chain and their autotuner: the x-pencil width
+and (FP64) the stream split are bitwise-neutral; every FP32-mixed choice
+(plane stages, where h is applied) agrees with the others and with FP64
+within the FP32-mixed tolerance; the autotuner's choice is a valid candidate;
+invalid choices are refused and leave the context as it was."""
+import itertools
 
 import numpy as np
 import pytest
 
+from conftest import rel_err
+
 pytestmark = pytest.mark.gpu
+
+FP32_PHI_TOL = 1e-5
 
 
 @pytest.fixture(scope="module")
@@ -14,42 +21,88 @@ def lfts(native_lib):
     return lfts_cpu_b200
 
 
-def _phi(lfts, precision, m, N, NA, cw, w2):
-    old = os.environ.get("LFTS_PENCIL_CW")
-    os.environ["LFTS_PENCIL_CW"] = str(cw)
-    try:
-        s = lfts.System(N, NA, 16.0, 100.0, 0.5, m, tuple(x / 16.0 for x in m), precision=precision)
-    finally:
-        if old is None:
-            del os.environ["LFTS_PENCIL_CW"]
-        else:
-            os.environ["LFTS_PENCIL_CW"] = old
-    assert s.tuning()[0] == cw
-    s.set_fields(w2)
-    lnq = s.calc_concs()
-    w = s.get_fields()
-    s.close()
-    return lnq, w
+def candidates(precision, m):
+    """Every tile combination, valid or not, for the context to accept or refuse."""
+    out = []
+    for cw, st, xh, two in itertools.product((8, 16, 32), (2, 3), (0, 1), (0, 1)):
+        if precision == 0 and (st != 2 or xh):
+            continue
+        if precision == 1 and two:
+            continue
+        out.append(dict(pencil_cw=cw, plane_stages=st, h_in_pencil=xh, two_streams=two))
+    return out
 
 
-@pytest.mark.parametrize("precision,m,N,NA", [(0, (32, 32, 32), 16, 8), (1, (32, 32, 32), 16, 8),
-                                              (0, (64, 64, 64), 12, 5), (1, (128, 128, 128), 10, 4)])
-def test_pencil_tile_width_is_bitwise_neutral(lfts, precision, m, N, NA):
+def valid(precision, m, t):
+    if precision == 0:
+        return True
+    if t["plane_stages"] == 3 and m[1] not in (64, 96, 128):
+        return False
+    if t["h_in_pencil"] and not (t["plane_stages"] == 3 and m[0] in (96, 128) and m[1] in (96, 128)):
+        return False
+    return True
+
+
+def run_all(lfts, precision, m, N, NA):
     M = int(np.prod(m))
     w2 = np.random.default_rng(M + N).normal(0.0, 0.7, 2 * M)
-    ref = _phi(lfts, precision, m, N, NA, 32, w2)
-    for cw in (8, 16):
-        lnq, w = _phi(lfts, precision, m, N, NA, cw, w2)
-        assert lnq == ref[0]
-        assert np.array_equal(w, ref[1])
+    s = lfts.System(N, NA, 16.0, 100.0, 0.5, m, tuple(x / 16.0 for x in m), precision=precision)
+    s.set_fields(w2)
+    tuned = s.tiles()
+    results = []
+    for t in candidates(precision, m):
+        if not valid(precision, m, t):
+            with pytest.raises(lfts.LftsError):
+                s.set_tiles(**t)
+            assert s.tiles() == (results[-1][0] if results else tuned)  # unchanged by the refusal
+            continue
+        s.set_tiles(**t)
+        assert s.tiles() == t
+        lnq = s.calc_concs()
+        results.append((t, lnq, s.get_fields()[2 * M:]))
+    s.close()
+    return tuned, results
 
 
-def test_autotuned_choices(lfts):
-    os.environ.pop("LFTS_PENCIL_CW", None)
-    for precision, m, stages in ((1, (128, 128, 128), 3), (1, (96, 96, 96), 3), (1, (64, 64, 64), 3),
-                                 (1, (48, 48, 48), 2), (0, (128, 128, 128), 2)):
+@pytest.mark.parametrize("m,N,NA", [((32, 32, 32), 16, 8), ((64, 64, 64), 12, 5), ((128, 128, 128), 10, 4)])
+def test_fp64_tiles_are_bitwise_neutral(lfts, m, N, NA):
+    tuned, res = run_all(lfts, 0, m, N, NA)
+    assert any(t == tuned for t, _, _ in res)
+    for t, lnq, phi in res[1:]:
+        assert lnq == res[0][1], t
+        assert np.array_equal(phi, res[0][2]), t
+
+
+@pytest.mark.parametrize("m,N,NA", [((32, 32, 32), 16, 8), ((64, 64, 64), 12, 5), ((96, 96, 96), 8, 3),
+                                    ((128, 128, 128), 10, 4)])
+def test_fp32_tiles_agree_within_tolerance(lfts, m, N, NA):
+    tuned, res = run_all(lfts, 1, m, N, NA)
+    assert any(t == tuned for t, _, _ in res)
+    M = int(np.prod(m))
+    w2 = np.random.default_rng(M + N).normal(0.0, 0.7, 2 * M)
+    s64 = lfts.System(N, NA, 16.0, 100.0, 0.5, m, tuple(x / 16.0 for x in m))
+    s64.set_fields(w2)
+    lnq64 = s64.calc_concs()
+    phi64 = s64.get_fields()[2 * M:]
+    s64.close()
+    for t, lnq, phi in res:
+        assert abs(lnq - lnq64) < FP32_PHI_TOL * max(1.0, abs(lnq64)), t
+        assert rel_err(phi, phi64) < FP32_PHI_TOL, t
+    # the pencil width alone changes no value
+    by_rest = {}
+    for t, lnq, phi in res:
+        key = (t["plane_stages"], t["h_in_pencil"])
+        if key in by_rest:
+            assert lnq == by_rest[key][0] and np.array_equal(phi, by_rest[key][1]), t
+        else:
+            by_rest[key] = (lnq, phi)
+
+
+def test_autotuned_choices_are_candidates(lfts):
+    for precision, m in ((1, (128, 128, 128)), (1, (96, 96, 96)), (1, (64, 64, 64)), (1, (48, 48, 48)),
+                         (0, (128, 128, 128)), (0, (32, 32, 32))):
         s = lfts.System(8, 3, 16.0, 100.0, 0.5, m, (4.0, 4.0, 4.0), precision=precision)
-        cw, st = s.tuning()
-        assert cw in (8, 16, 32)
-        assert st == stages
+        t = s.tiles()
+        assert t in candidates(precision, m) and valid(precision, m, t), (m, t)
+        assert s.tuning() == (t["pencil_cw"], t["plane_stages"])
         s.close()

@@ -195,3 +195,70 @@ def test_oracle_matches_reference_chain_edges(oracle_built, NA, NB):
     assert np.array_equal(a, b, equal_nan=True)  # NB = 0: the reference's mix diverges to NaN
     o.close()
     r.close()
+
+
+@pytest.mark.parametrize("m,NA,NB", [((16, 12, 20), 5, 7), ((8, 8, 8), 0, 4), ((12, 16, 8), 3, 0)])
+def test_scipy_bound_restatement_matches_oracle(Oracle, m, NA, NB):
+    """The scipy.fft calc_concs that bench.py times as the best-CPU-FFT bound
+    computes what the oracle computes."""
+    from scipy_path import ScipyConcs
+    L = (3.0, 2.5, 3.4)
+    M = int(np.prod(m))
+    w = np.zeros(4 * M)
+    w[:2 * M] = np.random.default_rng(M).normal(0.0, 1.0, 2 * M)
+    w2 = w.copy()
+    a = Oracle(NA, NB, m, L).calc_concs(w)
+    b = ScipyConcs(NA, NB, m, L, workers=2).calc_concs(w2)
+    assert abs(a - b) < 1e-13 * max(1.0, abs(a))
+    assert rel_err(w2[2 * M:], w[2 * M:]) < 1e-13
+
+
+def test_reference_full_step_matches_oracle(Oracle):
+    """The reference's own loop body as bench.py's reference arm times it
+    (langevin object on mt19937_64, step_wm, mix, the extra calc_concs) equals
+    the oracle fed the same noise, bitwise."""
+    import pyoracle
+    if not pyoracle.RefHarness.available():
+        pytest.skip("oracle/_ref not built (no reference tree on this machine)")
+    m, NA, NB, L, XbN, dt = (12, 16, 8), 5, 7, (3.0, 3.2, 2.4), 14.0, 0.5
+    M = int(np.prod(m))
+    sigma = 0.8
+    w = np.zeros(4 * M)
+    w[:2 * M] = np.random.default_rng(2).normal(0.0, 0.3, 2 * M)
+    wo = w.copy()
+    ref = pyoracle.RefSys(NA, NB, m, L)
+    lg = pyoracle.RefLangevin(99, sigma, M)
+    ref.mix(w)
+    o = Oracle(NA, NB, m, L)
+    o.mix(wo)
+    noise = np.empty(3 * M)
+    pyoracle.RefHarness.lib().ref_normal_stream(99, sigma, 3 * M, noise)
+    for st in range(2):
+        K, lnQ = lg.full_step(ref, w, XbN, dt)
+        Oracle.langevin_update(wo, noise[st * M:(st + 1) * M], noise[(st + 1) * M:(st + 2) * M], XbN, dt)
+        assert o.mix(wo) == K
+        assert o.calc_concs(wo) == lnQ
+        assert np.array_equal(w, wo)
+    lam = pyoracle.ref_lamellar(16.0, m)
+    expect = 16.0 * np.cos(2.0 * np.pi * (3.0 * np.arange(m[0]) / m[0]))
+    assert np.max(np.abs(lam[:M].reshape(m)[:, 0, 0] - expect)) < 1e-13
+    assert np.all(lam[M:] == 0.0)
+
+
+def test_oracle_matches_reference_at_config1_size(Oracle):
+    """The oracle against the reference at the plain-FP64 configuration's own
+    size (32^3, N=64, NA=32, seeded Gaussian start): calc_concs of the start
+    and the initial Anderson mix (fixture cfg1_32, compact)."""
+    g = golden("cfg1_32")
+    hdr = parse_header([str(s) for s in g["header"]])
+    m, L = tuple(hdr["m"]), tuple(hdr["L"])
+    M = int(np.prod(m))
+    stride = int(g["stride"])
+    w = np.zeros(4 * M)
+    w[:2 * M] = np.random.default_rng(int(g["field_seed"])).normal(0.0, 0.01, 2 * M)
+    o = Oracle(hdr["NA"], hdr["N"] - hdr["NA"], m, L, threads=4)
+    assert abs(o.calc_concs(w) - float(g["cc_lnQ"])) < 1e-14
+    assert rel_err(w[::stride][2 * M // stride + 1:], g["cc_w_s"][2 * M // stride + 1:]) < 1e-13
+    w[2 * M:] = 0.0
+    assert o.mix(w) == int(g["mix_K_unperturbed"])
+    o.close()

@@ -29,12 +29,12 @@ def _params(N, NA, m, L):
     return p
 
 
-@pytest.mark.parametrize("m,N,NA", [((64, 64, 64), 16, 6), ((12, 24, 16), 9, 4)])
-def test_noalloc_step_matches_context_step(native_lib, m, N, NA):
+def _calls(lib, m, N, NA, steps):
+    """Calls of the allocation-free step at monomer indices `steps`, each
+    checked against the context step on the same inputs."""
     import torch
 
     import lfts_cpu_b200 as lfts
-    lib = native_lib
     M = int(np.prod(m))
     L = (m[0] / 16.0, m[1] / 15.0, m[2] / 17.0)
     rng = np.random.default_rng(M + N)
@@ -42,7 +42,7 @@ def test_noalloc_step_matches_context_step(native_lib, m, N, NA):
     p = _params(N, NA, m, L)
     dev = torch.device("cuda:0")
     q_out = torch.empty(2 * M, dtype=torch.float64, device=dev)
-    for call, i in enumerate((1, N - 1)):  # two calls in a row, chain-1 h switches between them
+    for call, i in enumerate(steps):
         q_in = rng.uniform(0.2, 1.5, 2 * M)
         h = rng.uniform(0.5, 1.2, 2 * M)
         expect = ref.step_fwd(q_in, h, i)
@@ -60,6 +60,20 @@ def test_noalloc_step_matches_context_step(native_lib, m, N, NA):
     ref.close()
 
 
+# 128 x 32 x 64 fills the scratch exactly: 2 * 128 * 32 * 33 = LFTS_NOALLOC_MAX_SPECTRUM,
+# with the 128-point x twiddles and 128 per-plane partial sums at their limits
+@pytest.mark.parametrize("m,N,NA", [((64, 64, 64), 16, 6), ((12, 24, 16), 9, 4), ((128, 32, 64), 8, 3)])
+def test_noalloc_step_matches_context_step(native_lib, m, N, NA):
+    _calls(native_lib, m, N, NA, (1, N - 1))  # two calls in a row, chain-1 h switches between them
+
+
+def test_noalloc_step_after_a_larger_mesh(native_lib):
+    """The scratch keeps the last call's contents; a smaller mesh after the
+    largest one reads none of the larger call's tables or spectrum."""
+    _calls(native_lib, (128, 32, 64), 8, 3, (2,))
+    _calls(native_lib, (8, 12, 20), 7, 3, (1, 5))
+
+
 def test_noalloc_step_rejects_meshes_above_its_limit(native_lib):
     import torch
     lib = native_lib
@@ -69,4 +83,8 @@ def test_noalloc_step_rejects_meshes_above_its_limit(native_lib):
     rc = lib.lfts_step_fwd_noalloc(C.byref(p), ptr, ptr, ptr, 1, None)
     assert rc == 1  # LFTS_ERR_ARG, before any launch
     assert "limit" in lib.lfts_last_error_string().decode()
+    for bad in (0.0, -1.0, float("nan")):
+        q = _params(8, 4, (16, 16, 16), (2.0, bad, 2.0))
+        assert lib.lfts_step_fwd_noalloc(C.byref(q), ptr, ptr, ptr, 1, None) == 1
+        assert "box" in lib.lfts_last_error_string().decode()
     torch.cuda.synchronize()
