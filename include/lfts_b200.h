@@ -211,15 +211,15 @@ int lfts_get_propagators(lfts_ctx *ctx, double *q_host);
  * replicas of different meshes, each with its own parameters and noise
  * stream) advanced together.  The reference runs one system per process;
  * there is no counterpart.  Each replica is a context of its own (buffers,
- * tables, autotuned x-pencil width), computes exactly what a single
- * FP32-mixed context computes when fed the same noise (at 96^3 a context
- * created with LFTS_XH_CHAIN=0 in the environment: the ensemble keeps h in the
- * yz-plane kernel, single 96^3 contexts default to the x-pencil), and the ensemble
- * captures one Langevin step of every replica -- update, Anderson loop with
- * the least squares on the device, the extra calc_concs -- as one CUDA graph
- * launch (a WHILE node runs until every replica's loop has ended).
- * Replicas share N; meshes are 16, 24, 32, 48, 64 or 96 per side with square
- * yz planes. */
+ * tables), with tiles picked by timing the batched chain of its mesh group
+ * (lfts_ensemble_tiles), and computes exactly what a single FP32-mixed context
+ * with those tiles (lfts_set_tiles) computes when fed the same noise.  A run
+ * of Langevin steps of every replica -- update, Anderson loop with the least
+ * squares on the device, the extra calc_concs -- is one CUDA graph launch (up
+ * to 1024 steps per launch): a WHILE node over the steps holds a WHILE node
+ * over the Anderson iterations, which runs until every replica's loop has
+ * ended.  Replicas share N; meshes are 16, 24, 32, 48, 64 or 96 per side
+ * with square yz planes. */
 typedef struct lfts_ensemble lfts_ensemble;
 /* params[nrep], seeds[nrep]: the replicas' parameters and Philox streams. */
 int lfts_ensemble_create(const lfts_params *params, const unsigned long long *seeds, int nrep, int device,
@@ -235,8 +235,10 @@ int lfts_ensemble_get_fields(lfts_ensemble *ens, int r, double *w_host);
 int lfts_ensemble_mix(lfts_ensemble *ens, int maxIter, double tol, int *k_out, double *lnQ_out);
 /* nsteps Langevin steps of every replica (src/lfts_simulation.cc:69-76 per
  * replica: step_wm with on-device noise, mix, calc_concs); k_out[nsteps][nrep]
- * (may be null; reading it synchronises after every step), lnQ_out[nrep]
- * (may be null) after the last step.  The noise of replica r at step s is
+ * (may be null; recorded on the device), lnQ_out[nrep] (may be null) after
+ * the last step.  Every step runs: a replica whose mix fails stops its own
+ * Anderson loop in that step (and, with non-finite fields, in the later ones)
+ * while the others go on.  The noise of replica r at step s is
  * lfts_noise_philox(seeds[r], s, M, sigma_r); step 0 is the initial noise,
  * the first call's first step is step 1. */
 int lfts_ensemble_run(lfts_ensemble *ens, int nsteps, int maxIter, double tol, int *k_out, double *lnQ_out);

@@ -77,6 +77,17 @@ struct lfts_ctx {
     cudaGraph_t chain_graph = nullptr;
     cudaGraphExec_t chain_exec = nullptr;
     long long chain_kernels = 0;  // kernels in one replay of chain_exec
+    // the device-side Anderson loop (anderson_device.cuh): one graph launch per
+    // mix; LFTS_HOST_MIX=1 keeps the loop on the host
+    bool mix_on_device = true;
+    int mix_graph_state = 0;  // 0 not built, 1 built, -1 building failed (host loop)
+    void *d_mix = nullptr;    // MixState
+    double *d_lambda = nullptr;
+    int lambda_cap = 0;       // largest maxIter the lambda table covers
+    cudaGraph_t mix_graph = nullptr;
+    cudaGraphExec_t mix_exec = nullptr;
+    long long mix_body_kernels = 0;  // kernels per iteration of the mix graph's body
+    bool mix_pdl = false;            // the body kept the chain's programmatic edges
     bool use_pdl = true;      // LFTS_NO_PDL=1 in the environment turns it off
     bool two_streams = true;  // LFTS_ONE_STREAM=1 runs both chains in each launch
     long long launches = 0;

@@ -14,6 +14,7 @@
 #pragma once
 #include "fft_packed.cuh"
 #include "fft_plane3.cuh"
+#include "anderson_device.cuh"
 #include "field_kernels.cuh"
 #include "philox.cuh"
 
@@ -45,7 +46,7 @@ struct EnsRep {
     double DD[kRedWidth][kRedWidth];
 };
 
-__device__ __forceinline__ int ens_nh(int k) { return (k < kMaxHist + 1) ? k - 1 : kMaxHist; }
+__device__ __forceinline__ int ens_nh(int k) { return anderson_nh(k); }
 
 template <int NY, int NZ, int MODE>
 __global__ void __launch_bounds__(PlaneCCfg<float, NY, NZ>::NT, 1)
@@ -143,82 +144,6 @@ __global__ void __launch_bounds__(kRedThreads, 4) ens_conc_kernel(EnsRep *__rest
                                R.partials, blockIdx.x, R.red_blocks);
 }
 
-// GSL-style LU with partial pivoting and the two triangular solves
-// (src/anderson.cc:106-127) on one warp: lane i holds row i of the n x n
-// matrix (n <= kMaxHist) in registers and y[i].  Every matrix element goes
-// through the same operations in the same order as in the sequential
-// algorithm, each rounded separately (no fused multiply-adds), so x equals
-// the host's result bit for bit.  Returns false (all lanes) for an exactly
-// singular matrix.  x is valid in lane i for i < n.
-__device__ bool lu_solve_warp(double (&a)[kMaxHist], double y, double &x, int n)
-{
-    const int lane = threadIdx.x & 31;
-    int perm = lane;  // original row now at this position
-#pragma unroll
-    for (int j = 0; j < kMaxHist; j++) {
-        if (j >= n) break;
-        // first maximal |a_ij|, i >= j (scan in row order, as sequentially)
-        int piv = j;
-        double amax = fabs(__shfl_sync(0xffffffffu, a[j], j));
-        for (int i = j + 1; i < n; i++) {
-            const double v = fabs(__shfl_sync(0xffffffffu, a[j], i));
-            if (v > amax) {
-                amax = v;
-                piv = i;
-            }
-        }
-        if (piv != j) {
-            const int src = lane == j ? piv : (lane == piv ? j : lane);
-#pragma unroll
-            for (int k = 0; k < kMaxHist; k++) a[k] = __shfl_sync(0xffffffffu, a[k], src);
-            perm = __shfl_sync(0xffffffffu, perm, src);
-        }
-        if (j + 1 < n) {
-            const double ajj = __shfl_sync(0xffffffffu, a[j], j);
-            if (lane > j && lane < n) {
-                if (fabs(ajj) >= 2.2250738585072014e-308)
-                    a[j] = __dmul_rn(a[j], __ddiv_rn(1.0, ajj));
-                else
-                    a[j] = __ddiv_rn(a[j], ajj);
-            }
-#pragma unroll
-            for (int k = 0; k < kMaxHist; k++) {
-                if (k > j && k < n) {
-                    const double ajk = __shfl_sync(0xffffffffu, a[k], j);
-                    if (lane > j && lane < n) a[k] = __dsub_rn(a[k], __dmul_rn(a[j], ajk));
-                }
-            }
-        }
-    }
-    double diag = 1.0;
-#pragma unroll
-    for (int k = 0; k < kMaxHist; k++)
-        if (k == lane) diag = a[k];
-    if (__any_sync(0xffffffffu, lane < n && diag == 0.0)) return false;
-    // forward substitution (unit lower), x_j broadcast as it becomes final
-    double t = __shfl_sync(0xffffffffu, y, perm);
-#pragma unroll
-    for (int j = 0; j < kMaxHist; j++) {
-        if (j >= n) break;
-        const double xj = __shfl_sync(0xffffffffu, t, j);
-        if (lane > j && lane < n) t = __dsub_rn(t, __dmul_rn(a[j], xj));
-    }
-    // back substitution: row i subtracts a_ij x_j for j = i+1 .. n-1 in order
-    x = t;
-    for (int i = n - 1; i >= 0; i--) {
-        double ti = x;
-#pragma unroll
-        for (int j = 0; j < kMaxHist; j++) {
-            if (j > i && j < n) {
-                const double xj = __shfl_sync(0xffffffffu, x, j);
-                if (lane == i) ti = __dsub_rn(ti, __dmul_rn(a[j], xj));
-            }
-        }
-        if (lane == i) x = __ddiv_rn(ti, diag);
-    }
-    return true;
-}
-
 // One replica per block: the reduction of its dot products (as
 // reduce_partials_kernel, 256 threads, fixed order), then on one warp the
 // scalar part of the Anderson iteration (src/anderson.cc:35-89): the row
@@ -237,70 +162,7 @@ __global__ void __launch_bounds__(256) ens_reduce_solve_kernel(EnsRep *__restric
         }
         return;
     }
-    __shared__ double sh[32];
-    __shared__ double dd0[kRedWidth];
-    const int k = R.k, nh = ens_nh(k);
-    for (int m = 0; m <= nh; m++) {
-        double v = 0.0;
-        for (int b = threadIdx.x; b < R.red_blocks; b += blockDim.x) v += R.partials[(long long)b * kRedWidth + m];
-        v = block_sum(v, sh);
-        if (threadIdx.x == 0) dd0[m] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x >= 32) return;
-    const int lane = threadIdx.x;
-    if (lane <= nh) R.DD[0][lane] = dd0[lane];
-    __syncwarp();
-    const double DD00 = dd0[0];
-    bool ok = true;
-    if (k >= 2) {
-        // U_mn = DD00 - DD0m - DD0n + DD_nm (upper triangle), V_m = DD00 - DD0m
-        double a[kMaxHist];
-        const int m = lane + 1;  // this lane's row
-#pragma unroll
-        for (int c = 0; c < kMaxHist; c++) {
-            const int n = c + 1;
-            a[c] = 0.0;
-            if (m <= nh && n <= nh) {
-                const int lo = m < n ? m : n, hi = m < n ? n : m;
-                a[c] = __dadd_rn(__dsub_rn(__dsub_rn(DD00, dd0[hi]), dd0[lo]), R.DD[lo][hi]);
-            }
-        }
-        const double v = m <= nh ? __dsub_rn(DD00, dd0[m]) : 0.0;
-        double x = 0.0;
-        ok = lu_solve_warp(a, v, x, nh);
-        if (ok && lane < nh) R.coef[lane] = x;
-    }
-    __syncwarp();
-    if (lane == 0) {
-        R.simple = k < 2;
-        // err = (S1/M)^(1/2) (the reference takes pow(., 0.5); sqrt is the
-        // correctly rounded value of the same)
-        const double err = sqrt(__ddiv_rn(DD00, (double)R.M));
-        if (!isfinite(err)) {
-            // a NaN or infinite residual: stop before w+ is updated with it
-            // (the reference would update and then leave the loop, as NaN > tol
-            // is false)
-            R.nonfinite = 1;
-            R.stopped = 1;
-            R.go = 0;
-        } else if (!ok) {
-            R.singular = 1;
-            R.stopped = 1;
-            R.go = 0;
-        } else {
-            R.go = 1;
-            // the current deviation becomes history slot n (src/anderson.cc:82-89)
-            const int n = 1 + (k - 1) % kMaxHist;
-            R.DD[n][n] = DD00;
-            for (int c = 1; c < n; c++) R.DD[c][n] = dd0[c];
-            for (int c = n + 1; c <= nh; c++) R.DD[n][c] = dd0[c];
-            if (!(err > tol) || !(k + 1 < maxIter)) {
-                R.stopped = 1;
-                R.notconv = err > tol;  // the loop ends at the cap, above the tolerance
-            }
-        }
-    }
+    anderson_reduce_solve(R, R.partials, R.red_blocks, R.M, tol, maxIter);
 }
 
 // w+ update (src/anderson.cc:57-79): grid (max red_blocks, nrep); lambda[k] =
@@ -322,11 +184,31 @@ __global__ void __launch_bounds__(256) ens_update_kernel(EnsRep *__restrict__ re
 // After each body iteration: history rotation (src/anderson.cc:82-89) and
 // the next iteration number of every active replica; replicas whose extra
 // iteration just ran become idle.  Ends the WHILE loop when none is active.
-__global__ void ens_control_kernel(EnsRep *__restrict__ reps, int nrep, cudaGraphConditionalHandle loop)
+// guard[0] counts the body iterations of this mix; past `cap` (more than any
+// replica's loop can take: maxIter + 2) the loop ends regardless and the
+// replicas still active are marked (sticky bit 8), so no error in the
+// bookkeeping above can keep the WHILE node running.
+__global__ void ens_control_kernel(EnsRep *__restrict__ reps, int nrep, cudaGraphConditionalHandle loop, int *guard,
+                                   int cap)
 {
-    __shared__ int any;
-    if (threadIdx.x == 0) any = 0;
+    __shared__ int any, cut;
+    if (threadIdx.x == 0) {
+        any = 0;
+        cut = ++guard[0] >= cap;
+    }
     __syncthreads();
+    if (cut) {
+        for (int r = threadIdx.x; r < nrep; r += blockDim.x) {
+            EnsRep &R = reps[r];
+            if (!R.active) continue;
+            R.active = 0;
+            R.iters = R.k;
+            R.sticky |= 8;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) cudaGraphSetConditional(loop, 0u);
+        return;
+    }
     for (int r = threadIdx.x; r < nrep; r += blockDim.x) {
         EnsRep &R = reps[r];
         if (!R.active) continue;
@@ -349,9 +231,12 @@ __global__ void ens_control_kernel(EnsRep *__restrict__ reps, int nrep, cudaGrap
     if (threadIdx.x == 0) cudaGraphSetConditional(loop, any ? 1u : 0u);
 }
 
-// start of a mix: every replica active at iteration 1; with advance, the
-// Langevin step counter moves on (after this step's update used it)
-__global__ void ens_begin_kernel(EnsRep *__restrict__ reps, int nrep, long long *step, int advance)
+// start of a mix: every replica active at iteration 1, the iteration guard
+// at zero; with advance, the Langevin step counter moves on (after this
+// step's update used it); with set_inner (a mix nested in a run's step
+// loop), the mix's WHILE condition is raised again for this step
+__global__ void ens_begin_kernel(EnsRep *__restrict__ reps, int nrep, long long *step, int advance, int *guard,
+                                 int set_inner, cudaGraphConditionalHandle inner)
 {
     for (int r = threadIdx.x; r < nrep; r += blockDim.x) {
         EnsRep &R = reps[r];
@@ -359,7 +244,26 @@ __global__ void ens_begin_kernel(EnsRep *__restrict__ reps, int nrep, long long 
         R.active = 1;
         R.stopped = R.done = R.go = R.singular = R.notconv = R.nonfinite = 0;
     }
-    if (advance && threadIdx.x == 0) *step += 1;
+    if (threadIdx.x == 0) {
+        if (advance) *step += 1;
+        if (guard) guard[0] = 0;
+        if (set_inner) cudaGraphSetConditional(inner, 1u);
+    }
+}
+
+// end of one step of a run: records every replica's Anderson count for this
+// step (kbuf[step][replica]), counts the step and keeps the step loop going
+// while run[0] (steps done) < run[1] (steps asked for)
+__global__ void ens_step_end_kernel(const EnsRep *__restrict__ reps, int nrep, int *run, int *kbuf,
+                                    cudaGraphConditionalHandle outer)
+{
+    const int s = run[0];
+    for (int r = threadIdx.x; r < nrep; r += blockDim.x) kbuf[(long long)s * nrep + r] = reps[r].iters;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        run[0] = s + 1;
+        cudaGraphSetConditional(outer, s + 1 < run[1] ? 1u : 0u);
+    }
 }
 
 // clears the replicas' status bits at the start of a host call (mix or run)

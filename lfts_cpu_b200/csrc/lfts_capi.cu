@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/lfts_b200.h"
+#include "anderson_device.cuh"
 #include "ctx.h"
 #include "fft_dispatch.h"
 #include "field_kernels.cuh"
@@ -433,12 +434,19 @@ int set_pencil(lfts_ctx *c, int cw)
     return LFTS_OK;
 }
 
+// the captured chain and the Anderson-loop graph that holds it (rebuilt on
+// the next use with the new tiles)
 void drop_chain_graph(lfts_ctx *c)
 {
     if (c->chain_exec) cudaGraphExecDestroy(c->chain_exec);
     if (c->chain_graph) cudaGraphDestroy(c->chain_graph);
     c->chain_exec = nullptr;
     c->chain_graph = nullptr;
+    if (c->mix_exec) cudaGraphExecDestroy(c->mix_exec);
+    if (c->mix_graph) cudaGraphDestroy(c->mix_graph);
+    c->mix_exec = nullptr;
+    c->mix_graph = nullptr;
+    if (c->mix_graph_state == 1) c->mix_graph_state = 0;
 }
 
 // installs a tile choice (validated); the chain graph is captured anew
@@ -693,8 +701,10 @@ int calc_concs_sync(lfts_ctx *c, double *lnQ)
 }
 
 // anderson::mix (src/anderson.cc:24-93) with the history kept as a ring of
-// physical buffers addressed through the reference's logical slot numbers.
-int anderson_mix(lfts_ctx *c, int maxIter, double errTol, int *k_out)
+// physical buffers addressed through the reference's logical slot numbers:
+// the host-driven loop (one round trip per iteration for the dot products and
+// the least squares).  anderson_mix below runs the same loop on the device.
+int anderson_mix_host(lfts_ctx *c, int maxIter, double errTol, int *k_out)
 {
     const int nhMax = kMaxHist;
     const long long M = c->M;
@@ -767,6 +777,156 @@ int anderson_mix(lfts_ctx *c, int maxIter, double errTol, int *k_out)
     if (k_out) *k_out = k;
     c->have_concs = true;
     if (err > errTol) {  // the loop ended at maxIter
+        g_last_error = "Anderson mixing stopped at maxIter with the error above the tolerance";
+        return LFTS_ERR_NOTCONV;
+    }
+    return LFTS_OK;
+}
+
+// ---- the Anderson loop on the device ---------------------------------------------
+// One graph per context: begin -> WHILE { contour chain (the chain's own
+// launches, programmatic edges included), concentrations + dot products,
+// reduce + least squares (one warp, the host LU's operation order), w+
+// update, control }.  Bit for bit what anderson_mix_host computes; the host
+// sees the loop once per mix (state in, state out) instead of once per
+// iteration.
+template <typename T>
+int capture_mix_graph(lfts_ctx *c, cudaGraph_t *g_out)
+{
+    MixState *S = static_cast<MixState *>(c->d_mix);
+    cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    auto fail = [&](cudaError_t e, const char *what) {
+        cudaGraphDestroy(g);
+        cudaGetLastError();
+        return cuda_fail(e, what);
+    };
+    cudaGraphConditionalHandle loop;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&loop, g, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return fail(e, "conditional handle");
+    e = cudaStreamBeginCaptureToGraph(c->st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return fail(e, "mix graph capture");
+    mix_begin_kernel<<<1, 32, 0, c->st>>>(S);
+    cudaGraph_t cap = nullptr;
+    e = cudaStreamEndCapture(c->st, &cap);
+    if (e != cudaSuccess) return fail(e, "mix graph capture");
+    size_t nn = 1;
+    cudaGraphNode_t begin = nullptr;
+    e = cudaGraphGetNodes(g, &begin, &nn);
+    if (e != cudaSuccess) return fail(e, "mix graph nodes");
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = loop;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cond = nullptr;
+    e = cudaGraphAddNode(&cond, g, &begin, 1, &cp);
+    if (e != cudaSuccess) return fail(e, "mix graph WHILE node");
+    e = cudaStreamBeginCaptureToGraph(c->st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return fail(e, "mix graph body capture");
+    const long long launches0 = c->launches;
+    enqueue_chain_launches<T>(c);
+    mix_conc_kernel<T><<<stream_grid(c), kRedThreads, 0, c->st>>>(S, static_cast<const T *>(c->q), c->N, c->NA,
+                                                                    c->Qd);
+    mix_solve_kernel<<<1, 256, 0, c->st>>>(S);
+    mix_update_kernel<T><<<stream_grid(c), 256, 0, c->st>>>(S);
+    mix_control_kernel<<<1, 32, 0, c->st>>>(S, loop);
+    c->mix_body_kernels = c->launches - launches0 + 4;
+    c->launches = launches0;
+    e = cudaStreamEndCapture(c->st, &cap);
+    if (e != cudaSuccess) return fail(e, "mix graph body capture");
+    *g_out = g;
+    return LFTS_OK;
+}
+
+// builds the graph (with the chain's programmatic edges; without them if the
+// body refuses them); on failure the context keeps the host loop
+int ensure_mix_graph(lfts_ctx *c, int maxIter)
+{
+    if (c->mix_graph_state < 0) return LFTS_ERR_UNSUPPORTED;
+    if (!c->d_mix) CK(cudaMalloc(&c->d_mix, sizeof(MixState)));
+    if (maxIter + 2 > c->lambda_cap) {
+        // lambda_k = 1 - 0.9^k (src/anderson.cc:44), host pow as in anderson_mix_host
+        const int cap = std::max(maxIter + 2, 256);
+        std::vector<double> lam(cap);
+        for (int k = 0; k < cap; k++) lam[k] = 1.0 - std::pow(0.9, double(k));
+        cudaFree(c->d_lambda);
+        c->d_lambda = nullptr;
+        CK(cudaMalloc(&c->d_lambda, sizeof(double) * cap));
+        CK(cudaMemcpy(c->d_lambda, lam.data(), sizeof(double) * cap, cudaMemcpyHostToDevice));
+        c->lambda_cap = cap;
+    }
+    if (c->mix_graph_state == 1) return LFTS_OK;
+    const bool pdl = c->use_pdl;
+    int rc = LFTS_ERR_CUDA;
+    for (int attempt = 0; attempt < 2 && rc; attempt++) {
+        c->use_pdl = pdl && attempt == 0;
+        cudaGraph_t g = nullptr;
+        rc = c->prec == LFTS_FP64 ? capture_mix_graph<double>(c, &g) : capture_mix_graph<float>(c, &g);
+        if (!rc) {
+            cudaError_t e = cudaGraphInstantiate(&c->mix_exec, g, 0);
+            if (e == cudaSuccess) e = cudaGraphUpload(c->mix_exec, c->st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+            if (e != cudaSuccess) {
+                if (c->mix_exec) cudaGraphExecDestroy(c->mix_exec);
+                c->mix_exec = nullptr;
+                cudaGraphDestroy(g);
+                cudaGetLastError();
+                rc = cuda_fail(e, "mix graph instantiate");
+            } else {
+                c->mix_graph = g;
+                c->mix_pdl = c->use_pdl;
+            }
+        }
+    }
+    c->use_pdl = pdl;
+    c->mix_graph_state = rc ? -1 : 1;
+    return rc;
+}
+
+int anderson_mix(lfts_ctx *c, int maxIter, double errTol, int *k_out)
+{
+    if (!c->mix_on_device || maxIter < 2 || ensure_mix_graph(c, maxIter) != LFTS_OK)
+        return anderson_mix_host(c, maxIter, errTol, k_out);
+    MixState h{};
+    h.M = c->M;
+    h.red_blocks = c->red_blocks;
+    h.maxIter = maxIter;
+    h.tol = errTol;
+    h.w = c->w;
+    h.partials = c->partials;
+    h.lambda = c->d_lambda;
+    for (int i = 0; i < kRedWidth; i++) {
+        h.Dh[i] = c->Dh[i];
+        h.wh[i] = c->wh[i];
+        h.phys[i] = c->phys[i];
+    }
+    h.cur = c->cur;
+    MixState *S = static_cast<MixState *>(c->d_mix);
+    CK(cudaMemcpyAsync(S, &h, sizeof(MixState), cudaMemcpyHostToDevice, c->st));
+    CK(cudaGraphLaunch(c->mix_exec, c->st));
+    CK(cudaMemcpyAsync(&h, S, sizeof(MixState), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (int i = 0; i < kRedWidth; i++) c->phys[i] = h.phys[i];
+    c->cur = h.cur;
+    std::memcpy(c->DD, h.DD, sizeof(c->DD));
+    const bool failed = h.nonfinite || h.singular;
+    c->mix_iters += h.iters - 1 - (failed ? 1 : 0);
+    c->mix_calls++;
+    c->launches += (long long)(h.iters - 1) * c->mix_body_kernels + 1;
+    if (h.nonfinite) {
+        g_last_error = "NaN or infinite Anderson residual (non-finite fields or concentrations)";
+        if (k_out) *k_out = h.iters;
+        return LFTS_ERR_NONFINITE;
+    }
+    if (h.singular) {
+        g_last_error = "Anderson least-squares matrix is singular";
+        return LFTS_ERR_SINGULAR;
+    }
+    if (k_out) *k_out = h.iters;
+    c->have_concs = true;
+    if (h.notconv) {
         g_last_error = "Anderson mixing stopped at maxIter with the error above the tolerance";
         return LFTS_ERR_NOTCONV;
     }
@@ -914,8 +1074,9 @@ void ctx_free(lfts_ctx *c)
     cudaFree(c->sf_buf);
     cudaFree(c->adj_partial);
     cudaFree(c->adj_buf);
-    if (c->chain_exec) cudaGraphExecDestroy(c->chain_exec);
-    if (c->chain_graph) cudaGraphDestroy(c->chain_graph);
+    drop_chain_graph(c);
+    cudaFree(c->d_mix);
+    cudaFree(c->d_lambda);
     if (c->st1) cudaStreamSynchronize(c->st1);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
@@ -1136,6 +1297,8 @@ int lfts_create(const lfts_params *p, int precision, int device, lfts_ctx **out)
     if (const char *e = getenv("LFTS_NO_PDL")) c->use_pdl = !(e[0] == '1');
     if (const char *e = getenv("LFTS_ONE_STREAM")) c->two_streams = !(e[0] == '1');
     if (const char *e = getenv("LFTS_NO_GRAPH")) c->use_graph = !(e[0] == '1');
+    if (const char *e = getenv("LFTS_HOST_MIX")) c->mix_on_device = !(e[0] == '1');
+    if (!c->use_graph) c->mix_on_device = false;
     int rc = LFTS_OK;
     auto fail = [&](int code) {
         ctx_free(c);

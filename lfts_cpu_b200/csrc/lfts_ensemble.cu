@@ -157,8 +157,13 @@ struct lfts_ensemble {
     int lambda_n = 0;
     int max_blocks = 0;           // largest reduction grid of any replica
     // graphs, built for one (maxIter, tol)
-    cudaGraph_t g_mix = nullptr, g_step = nullptr;
-    cudaGraphExec_t x_mix = nullptr, x_step = nullptr;
+    cudaGraph_t g_mix = nullptr, g_run = nullptr;
+    cudaGraphExec_t x_mix = nullptr, x_run = nullptr;
+    int *d_guard = nullptr;  // body iterations of the current mix (the WHILE node's guard)
+    int guard_cap = 0;
+    int *d_run = nullptr;    // steps done, steps asked for (the run graph's step loop)
+    int *d_kbuf = nullptr;   // Anderson counts of a run, [kbuf_steps][nrep]
+    int kbuf_steps = 0;
     int g_maxIter = -1;
     double g_tol = -1.0;
     long long launches = 0;
@@ -205,88 +210,152 @@ int enqueue_body(lfts_ensemble *e, int maxIter, double tol, cudaGraphConditional
     ens_conc_kernel<<<dim3(e->max_blocks, e->nrep), kRedThreads, 0, e->s0>>>(e->d_reps);
     ens_reduce_solve_kernel<<<e->nrep, 256, 0, e->s0>>>(e->d_reps, tol, maxIter);
     ens_update_kernel<<<dim3(e->max_blocks, e->nrep), 256, 0, e->s0>>>(e->d_reps, e->d_lambda);
-    ens_control_kernel<<<1, 256, 0, e->s0>>>(e->d_reps, e->nrep, loop);
+    ens_control_kernel<<<1, 256, 0, e->s0>>>(e->d_reps, e->nrep, loop, e->d_guard, e->guard_cap);
     e->launches += 5;
     EK(cudaGetLastError());
     return LFTS_OK;
 }
 
-// [Langevin update ->] begin -> WHILE(body)
-int build_graph(lfts_ensemble *e, bool langevin, int maxIter, double tol, cudaGraph_t *g_out, cudaGraphExec_t *x_out)
+// A WHILE node running enqueue_body (the Anderson loop of every replica),
+// added to graph g after node `dep` (null: no dependency); *loop_out is its
+// handle, created in g.
+int add_mix_loop(lfts_ensemble *e, cudaGraph_t g, cudaGraphNode_t dep, int maxIter, double tol,
+                 cudaGraphConditionalHandle loop, cudaGraphNode_t *node_out)
 {
-    cudaGraph_t g = nullptr;
-    EK(cudaGraphCreate(&g, 0));
-    cudaGraphConditionalHandle loop;
-    EK(cudaGraphConditionalHandleCreate(&loop, g, 1, cudaGraphCondAssignDefault));
-
-    // prologue, captured into g
-    EK(cudaStreamBeginCaptureToGraph(e->s0, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    if (langevin) {
-        long long maxM = 0;
-        for (const EnsRep &r : e->h_reps) maxM = std::max(maxM, r.M);
-        const int lb = (int)std::min<long long>((maxM + 255) / 256, 1184);
-        ens_langevin_kernel<<<dim3(lb, e->nrep), 256, 0, e->s0>>>(e->d_reps, e->d_step);
-    }
-    ens_begin_kernel<<<1, 256, 0, e->s0>>>(e->d_reps, e->nrep, e->d_step, langevin ? 1 : 0);
-    cudaGraph_t captured = nullptr;
-    cudaError_t ce = cudaStreamEndCapture(e->s0, &captured);
-    if (ce != cudaSuccess) {
-        cudaGraphDestroy(g);
-        EK(ce);
-    }
-    // the prologue's last node: the one without dependents
-    size_t nn = 0;
-    EK(cudaGraphGetNodes(g, nullptr, &nn));
-    std::vector<cudaGraphNode_t> nodes(nn);
-    EK(cudaGraphGetNodes(g, nodes.data(), &nn));
-    cudaGraphNode_t last = nullptr;
-    for (cudaGraphNode_t n : nodes) {
-        size_t nd = 0;
-        EK(cudaGraphNodeGetDependentNodes(n, nullptr, &nd));
-        if (nd == 0) last = n;
-    }
-
     cudaGraphNodeParams cp = {};
     cp.type = cudaGraphNodeTypeConditional;
     cp.conditional.handle = loop;
     cp.conditional.type = cudaGraphCondTypeWhile;
     cp.conditional.size = 1;
-    cudaGraphNode_t cond = nullptr;
-    EK(cudaGraphAddNode(&cond, g, &last, last ? 1 : 0, &cp));
+    EK(cudaGraphAddNode(node_out, g, &dep, dep ? 1 : 0, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     EK(cudaStreamBeginCaptureToGraph(e->s0, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     int rc = enqueue_body(e, maxIter, tol, loop);
     cudaGraph_t body_out = nullptr;
-    ce = cudaStreamEndCapture(e->s0, &body_out);
-    if (rc) {
-        cudaGraphDestroy(g);
-        return rc;
+    cudaError_t ce = cudaStreamEndCapture(e->s0, &body_out);
+    if (rc) return rc;
+    EK(ce);
+    return LFTS_OK;
+}
+
+// the node of g without dependents (the end of a captured prologue)
+int last_node(cudaGraph_t g, cudaGraphNode_t *out)
+{
+    size_t nn = 0;
+    EK(cudaGraphGetNodes(g, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    EK(cudaGraphGetNodes(g, nodes.data(), &nn));
+    *out = nullptr;
+    for (cudaGraphNode_t n : nodes) {
+        size_t nd = 0;
+        EK(cudaGraphNodeGetDependentNodes(n, nullptr, &nd));
+        if (nd == 0) *out = n;
     }
-    if (ce != cudaSuccess) {
-        cudaGraphDestroy(g);
-        EK(ce);
-    }
+    return LFTS_OK;
+}
+
+int finish_graph(lfts_ensemble *e, cudaGraph_t g, cudaGraphExec_t *x_out)
+{
     cudaGraphExec_t x = nullptr;
-    ce = cudaGraphInstantiate(&x, g, 0);
-    if (ce != cudaSuccess) {
-        cudaGraphDestroy(g);
-        EK(ce);
-    }
+    EK(cudaGraphInstantiate(&x, g, 0));
     EK(cudaGraphUpload(x, e->s0));
     EK(cudaStreamSynchronize(e->s0));
-    *g_out = g;
     *x_out = x;
+    return LFTS_OK;
+}
+
+void langevin_launch(lfts_ensemble *e)
+{
+    long long maxM = 0;
+    for (const EnsRep &r : e->h_reps) maxM = std::max(maxM, r.M);
+    const int lb = (int)std::min<long long>((maxM + 255) / 256, 1184);
+    ens_langevin_kernel<<<dim3(lb, e->nrep), 256, 0, e->s0>>>(e->d_reps, e->d_step);
+}
+
+// the mix graph: begin -> WHILE(body)
+int build_mix_graph(lfts_ensemble *e, int maxIter, double tol, cudaGraph_t *g_out, cudaGraphExec_t *x_out)
+{
+    cudaGraph_t g = nullptr;
+    EK(cudaGraphCreate(&g, 0));
+    auto fail = [&](int rc) {
+        cudaGraphDestroy(g);
+        return rc;
+    };
+    cudaGraphConditionalHandle loop;
+    if (cudaGraphConditionalHandleCreate(&loop, g, 1, cudaGraphCondAssignDefault) != cudaSuccess)
+        return fail(LFTS_ERR_CUDA);
+    if (cudaStreamBeginCaptureToGraph(e->s0, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return fail(LFTS_ERR_CUDA);
+    ens_begin_kernel<<<1, 256, 0, e->s0>>>(e->d_reps, e->nrep, e->d_step, 0, e->d_guard, 0, 0);
+    cudaGraph_t captured = nullptr;
+    if (cudaStreamEndCapture(e->s0, &captured) != cudaSuccess) return fail(LFTS_ERR_CUDA);
+    cudaGraphNode_t last = nullptr, cond = nullptr;
+    int rc = last_node(g, &last);
+    if (!rc) rc = add_mix_loop(e, g, last, maxIter, tol, loop, &cond);
+    if (!rc) rc = finish_graph(e, g, x_out);
+    if (rc) return fail(rc);
+    *g_out = g;
+    return LFTS_OK;
+}
+
+// the run graph, one launch for a whole run of Langevin steps:
+//   WHILE (steps done < steps asked) {
+//       Langevin update -> begin (raises the mix condition) -> WHILE(mix body) -> step end
+//   }
+// the step loop's handle belongs to the top graph, the mix loop's to the
+// step loop's body
+int build_run_graph(lfts_ensemble *e, int maxIter, double tol, cudaGraph_t *g_out, cudaGraphExec_t *x_out)
+{
+    cudaGraph_t g = nullptr;
+    EK(cudaGraphCreate(&g, 0));
+    auto fail = [&](int rc) {
+        cudaGraphDestroy(g);
+        return rc;
+    };
+    cudaGraphConditionalHandle outer;
+    if (cudaGraphConditionalHandleCreate(&outer, g, 1, cudaGraphCondAssignDefault) != cudaSuccess)
+        return fail(LFTS_ERR_CUDA);
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = outer;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t outer_node = nullptr;
+    if (cudaGraphAddNode(&outer_node, g, nullptr, 0, &cp) != cudaSuccess) return fail(LFTS_ERR_CUDA);
+    cudaGraph_t steps = cp.conditional.phGraph_out[0];
+    cudaGraphConditionalHandle inner;
+    if (cudaGraphConditionalHandleCreate(&inner, steps, 1, cudaGraphCondAssignDefault) != cudaSuccess)
+        return fail(LFTS_ERR_CUDA);
+    // step prologue: Langevin update of every replica, begin of the mix
+    if (cudaStreamBeginCaptureToGraph(e->s0, steps, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+        cudaSuccess)
+        return fail(LFTS_ERR_CUDA);
+    langevin_launch(e);
+    ens_begin_kernel<<<1, 256, 0, e->s0>>>(e->d_reps, e->nrep, e->d_step, 1, e->d_guard, 1, inner);
+    cudaGraph_t captured = nullptr;
+    if (cudaStreamEndCapture(e->s0, &captured) != cudaSuccess) return fail(LFTS_ERR_CUDA);
+    cudaGraphNode_t last = nullptr, mix = nullptr;
+    int rc = last_node(steps, &last);
+    if (!rc) rc = add_mix_loop(e, steps, last, maxIter, tol, inner, &mix);
+    if (rc) return fail(rc);
+    // step end, after the mix loop
+    if (cudaStreamBeginCaptureToGraph(e->s0, steps, &mix, nullptr, 1, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return fail(LFTS_ERR_CUDA);
+    ens_step_end_kernel<<<1, 256, 0, e->s0>>>(e->d_reps, e->nrep, e->d_run, e->d_kbuf, outer);
+    if (cudaStreamEndCapture(e->s0, &captured) != cudaSuccess) return fail(LFTS_ERR_CUDA);
+    if ((rc = finish_graph(e, g, x_out))) return fail(rc);
+    *g_out = g;
     return LFTS_OK;
 }
 
 void drop_graphs(lfts_ensemble *e)
 {
     if (e->x_mix) cudaGraphExecDestroy(e->x_mix);
-    if (e->x_step) cudaGraphExecDestroy(e->x_step);
+    if (e->x_run) cudaGraphExecDestroy(e->x_run);
     if (e->g_mix) cudaGraphDestroy(e->g_mix);
-    if (e->g_step) cudaGraphDestroy(e->g_step);
-    e->x_mix = e->x_step = nullptr;
-    e->g_mix = e->g_step = nullptr;
+    if (e->g_run) cudaGraphDestroy(e->g_run);
+    e->x_mix = e->x_run = nullptr;
+    e->g_mix = e->g_run = nullptr;
 }
 
 int ensure_graphs(lfts_ensemble *e, int maxIter, double tol)
@@ -301,8 +370,9 @@ int ensure_graphs(lfts_ensemble *e, int maxIter, double tol)
     EK(cudaMalloc(&e->d_lambda, sizeof(double) * lam.size()));
     EK(cudaMemcpy(e->d_lambda, lam.data(), sizeof(double) * lam.size(), cudaMemcpyHostToDevice));
     e->lambda_n = (int)lam.size();
-    int rc = build_graph(e, false, maxIter, tol, &e->g_mix, &e->x_mix);
-    if (!rc) rc = build_graph(e, true, maxIter, tol, &e->g_step, &e->x_step);
+    e->guard_cap = maxIter + 2;
+    int rc = build_mix_graph(e, maxIter, tol, &e->g_mix, &e->x_mix);
+    if (!rc) rc = build_run_graph(e, maxIter, tol, &e->g_run, &e->x_run);
     if (rc) {
         drop_graphs(e);
         return rc;
@@ -357,7 +427,7 @@ int tune_groups(lfts_ensemble *e)
     const char *fcw = std::getenv("LFTS_PENCIL_CW");
     const int cw_forced = fcw ? std::atoi(fcw) : 0;
     // every replica active, so that the batched kernels do their work
-    ens_begin_kernel<<<1, 256, 0, e->s0>>>(e->d_reps, e->nrep, e->d_step, 0);
+    ens_begin_kernel<<<1, 256, 0, e->s0>>>(e->d_reps, e->nrep, e->d_step, 0, nullptr, 0, 0);
     EK(cudaStreamSynchronize(e->s0));
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     EK(cudaEventCreate(&e0));
@@ -426,7 +496,7 @@ int read_back(lfts_ensemble *e, int *k_out, double *lnQ_out)
         const EnsRep &R = e->h_reps[r];
         if (k_out) k_out[r] = R.iters;
         const int s = (R.sticky & 4) ? LFTS_ERR_NONFINITE : (R.sticky & 2) ? LFTS_ERR_SINGULAR
-                                                          : (R.sticky & 1) ? LFTS_ERR_NOTCONV : LFTS_OK;
+                                                          : (R.sticky & 9) ? LFTS_ERR_NOTCONV : LFTS_OK;
         e->status[r] = s;
         if (rank(s) > rank(worst)) {
             worst = s;
@@ -559,6 +629,11 @@ int lfts_ensemble_create(const lfts_params *params, const unsigned long long *se
         cudaMalloc(&e->d_step, sizeof(long long)) != cudaSuccess ||
         cudaMemcpy(e->d_step, &step1, sizeof(long long), cudaMemcpyHostToDevice) != cudaSuccess)
         return fail(LFTS_ERR_NOMEM);
+    e->kbuf_steps = 1024;
+    if (cudaMalloc(&e->d_guard, sizeof(int)) != cudaSuccess || cudaMemset(e->d_guard, 0, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&e->d_run, 2 * sizeof(int)) != cudaSuccess || cudaMemset(e->d_run, 0, 2 * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&e->d_kbuf, sizeof(int) * (size_t)e->kbuf_steps * nrep) != cudaSuccess)
+        return fail(LFTS_ERR_NOMEM);
     int rc = tune_groups(e);
     if (rc) return fail(rc);
     *out = e;
@@ -581,6 +656,9 @@ int lfts_ensemble_destroy(lfts_ensemble *e)
     cudaFree(e->d_reps);
     cudaFree(e->d_step);
     cudaFree(e->d_lambda);
+    cudaFree(e->d_guard);
+    cudaFree(e->d_run);
+    cudaFree(e->d_kbuf);
     for (lfts_ctx *c : e->rep) lfts_destroy(c);
     delete e;
     return LFTS_OK;
@@ -620,14 +698,16 @@ int lfts_ensemble_run(lfts_ensemble *e, int nsteps, int maxIter, double tol, int
     int rc = ensure_graphs(e, maxIter, tol);
     if (rc) return rc;
     ens_clear_status_kernel<<<1, 256, 0, e->s0>>>(e->d_reps, e->nrep);
-    for (int s = 0; s < nsteps; s++) {
-        EK(cudaGraphLaunch(e->x_step, e->s0));
-        if (k_out) {
-            // a mix that stopped at the cap completes its step and the run goes
-            // on (the reference's loop does); any other failure ends the run
-            rc = read_back(e, k_out + (long long)s * e->nrep, nullptr);
-            if (rc && rc != LFTS_ERR_NOTCONV) return rc;
-        }
+    // one graph launch runs up to kbuf_steps steps (the step loop is a WHILE
+    // node on the device); the Anderson counts come back once per launch
+    for (int s0 = 0; s0 < nsteps; s0 += e->kbuf_steps) {
+        const int n = std::min(e->kbuf_steps, nsteps - s0);
+        const int run[2] = {0, n};
+        EK(cudaMemcpyAsync(e->d_run, run, sizeof(run), cudaMemcpyHostToDevice, e->s0));
+        EK(cudaGraphLaunch(e->x_run, e->s0));
+        if (k_out)
+            EK(cudaMemcpyAsync(k_out + (long long)s0 * e->nrep, e->d_kbuf, sizeof(int) * (size_t)n * e->nrep,
+                               cudaMemcpyDeviceToHost, e->s0));
     }
     return read_back(e, nullptr, lnQ_out);
 }

@@ -16,6 +16,10 @@ struct lfts_rng {
 
 extern "C" {
 
+// z_inf of the discrete Gaussian chain on the mesh (src/lfts_params.cc:122-142):
+// the same terms in the same order and the same variable roles (R0dL, ell,
+// the t-sum, the tail correction), so that chi_b N comes out bit for bit equal
+// to the reference's for the same input header.
 double lfts_z_inf_discrete(const double L[3], const int m[3], int N, double Nbar, int tmax)
 {
     const double pi = 3.14159265358979323846;

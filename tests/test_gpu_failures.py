@@ -12,6 +12,8 @@
 each for single contexts in both precisions and for a 2-replica ensemble,
 whose device-side loop ends at its cap and reports per replica while the
 healthy replica runs on unchanged."""
+import os
+
 import numpy as np
 import pytest
 
@@ -29,13 +31,30 @@ def lfts(native_lib):
     return lfts_cpu_b200
 
 
+@pytest.fixture(params=["device", "host"])
+def system(lfts, request):
+    """A 16^3 context with its Anderson loop on the device (the default) or
+    on the host (LFTS_HOST_MIX=1)."""
+    def make(precision):
+        old = os.environ.get("LFTS_HOST_MIX")
+        os.environ["LFTS_HOST_MIX"] = "1" if request.param == "host" else "0"
+        try:
+            return lfts.System(N, NA, 12.0, 50.0, 0.5, M3, L, precision=precision)
+        finally:
+            if old is None:
+                del os.environ["LFTS_HOST_MIX"]
+            else:
+                os.environ["LFTS_HOST_MIX"] = old
+    return make
+
+
 def rough(seed=3):
     return np.random.default_rng(seed).normal(0.0, 1.0, 2 * M)
 
 
 @pytest.mark.parametrize("precision", [0, 1])
-def test_nan_field_reports_nonfinite(lfts, precision):
-    s = lfts.System(N, NA, 12.0, 50.0, 0.5, M3, L, precision=precision)
+def test_nan_field_reports_nonfinite(lfts, system, precision):
+    s = system(precision)
     w2 = rough()
     w2[123] = np.nan
     s.set_fields(w2)
@@ -47,9 +66,9 @@ def test_nan_field_reports_nonfinite(lfts, precision):
 
 
 @pytest.mark.parametrize("precision", [0, 1])
-def test_iteration_cap_reports_notconv(lfts, oracle_built, precision):
+def test_iteration_cap_reports_notconv(lfts, system, oracle_built, precision):
     from pyoracle import Oracle
-    s = lfts.System(N, NA, 12.0, 50.0, 0.5, M3, L, precision=precision)
+    s = system(precision)
     w2 = rough()
     s.set_fields(w2)
     k = s.mix(max_iter=3)
@@ -58,7 +77,7 @@ def test_iteration_cap_reports_notconv(lfts, oracle_built, precision):
         s.mix(max_iter=3, strict=True)
     assert e.value.status == lfts.LFTS_ERR_NOTCONV
     # the fields after the first capped mix are the reference's (oracle, same cap)
-    s2 = lfts.System(N, NA, 12.0, 50.0, 0.5, M3, L, precision=precision)
+    s2 = system(precision)
     s2.set_fields(w2)
     s2.mix(max_iter=3)
     o = Oracle(NA, N - NA, M3, L)
@@ -78,8 +97,8 @@ def test_iteration_cap_reports_notconv(lfts, oracle_built, precision):
 
 
 @pytest.mark.parametrize("precision", [0, 1])
-def test_singular_system_reports_singular(lfts, precision):
-    s = lfts.System(N, NA, 12.0, 50.0, 0.5, M3, L, precision=precision)
+def test_singular_system_reports_singular(lfts, system, precision):
+    s = system(precision)
     s.set_fields(np.zeros(2 * M))
     with pytest.raises(lfts.LftsError) as e:
         s.mix(max_iter=10, tol=-1.0)
