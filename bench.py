@@ -564,6 +564,7 @@ def main(argv=None):
     # counts per step; the rest is host round trips, launch gaps and the
     # once-per-step kernels
     part_chain, part_conc, part_upd = fp32_sys.profile_iteration(5)
+    tiles32 = fp32_sys.tiles()
     fp32_sys.close()
     fp64 = run_precision(lfts, lfts.LFTS_FP64, args.steps, args.warmup, rank, device, torch, None)
     fp64.pop("system").close()
@@ -640,6 +641,7 @@ def main(argv=None):
             "mesh_point_contour_steps_per_s": fp32["calc_concs_per_step"] * M * (N - 1) * 1e3 / ms32,
             "hbm_gbs_algorithmic_step": step_alg / (ms32 * 1e-3) / 1e9,
             "step_split": split_info,
+            "tiles": tiles32,
             "fp64": {"value": world * 1e3 / ms64, "ms_per_step": ms64, "mean_anderson_K": K64,
                      "e2e": {"value": world * 1e3 / e2e64, "unit": "steps/s",
                              "h2d_bytes_per_step": fp64["h2d_bytes_per_step"],

@@ -185,6 +185,10 @@ typedef struct lfts_tiles {
     int h_in_pencil;   /* FP32-mixed: h and the propagator stores in the x-pencil kernel and g in the
                           yz-plane kernel (1; 96- and 128-point x lines, 3 stages), or all in the yz-plane (0) */
     int two_streams;   /* FP64: each chain on its own stream (1) or both chains in every launch (0) */
+    int phi_in_chain;  /* with h_in_pencil: the concentration sums formed in the x-pencil from the
+                          middle of the chain on (each new slot times its already stored partner,
+                          FP32 sums; the later slots are then not stored) (1), or by a separate
+                          pass over all N stored slots (0) */
 } lfts_tiles;
 /* lfts_create picks the tiles by timing the whole contour chain for every
  * valid combination on the context's own buffers and keeping the fastest,

@@ -230,8 +230,9 @@ class System:
         check(lib().lfts_get_tiles(self._h, C.byref(t)), "lfts_get_tiles")
         return t.as_dict()
 
-    def set_tiles(self, pencil_cw: int, plane_stages: int, h_in_pencil: int = 0, two_streams: int = 0) -> None:
-        t = Tiles(int(pencil_cw), int(plane_stages), int(h_in_pencil), int(two_streams))
+    def set_tiles(self, pencil_cw: int, plane_stages: int, h_in_pencil: int = 0, two_streams: int = 0,
+                  phi_in_chain: int = 0) -> None:
+        t = Tiles(int(pencil_cw), int(plane_stages), int(h_in_pencil), int(two_streams), int(phi_in_chain))
         check(lib().lfts_set_tiles(self._h, C.byref(t)), "lfts_set_tiles")
 
     def profile_chain(self):

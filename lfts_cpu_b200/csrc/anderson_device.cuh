@@ -208,6 +208,19 @@ __global__ void __launch_bounds__(kRedThreads, 4)
                            hist, S->partials, blockIdx.x, gridDim.x);
 }
 
+// the same from the concentration sums the contour chain formed (PENCIL_HA)
+static __global__ void __launch_bounds__(kRedThreads, 4)
+    mix_conc_acc_kernel(const MixState *__restrict__ S, const float *__restrict__ acc, const float *__restrict__ h,
+                        int N, const double *__restrict__ Qd)
+{
+    const int nh = anderson_nh(S->k);
+    HistPtrs hist{};
+    for (int m = 1; m <= nh; m++) hist.p[m - 1] = S->Dh[S->phys[m]];
+    const long long M = S->M;
+    concentrations_acc_body(acc, h, M, N, S->w + 2 * M, S->w + 3 * M, Qd, static_cast<float *>(S->Dh[S->cur]), nh,
+                            hist, S->partials, blockIdx.x, gridDim.x);
+}
+
 static __global__ void __launch_bounds__(256) mix_solve_kernel(MixState *S)
 {
     anderson_reduce_solve(*S, S->partials, S->red_blocks, S->M, S->tol, S->maxIter);

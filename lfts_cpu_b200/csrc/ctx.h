@@ -73,6 +73,8 @@ struct lfts_ctx {
     bool have_concs = false;
     bool packed = false;      // FP32: both chains as one complex field (fft_packed.cuh)
     bool xh_chain = false;    // FP32 128^3: h and the q stores in the x-pencil (enqueue_chain_launches)
+    bool phi_in_chain = false;  // with xh_chain: the concentration sums formed in the chain (PENCIL_HA)
+    void *acc = nullptr;      // their (A, B) sums per mesh point, FP32 pairs
     bool use_graph = true;    // LFTS_NO_GRAPH=1: launch the chain kernel by kernel
     cudaGraph_t chain_graph = nullptr;
     cudaGraphExec_t chain_exec = nullptr;

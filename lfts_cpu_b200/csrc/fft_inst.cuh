@@ -54,8 +54,11 @@ static void fill_pencil(PencilKernels<T> *o)
         o->fn[PENCIL_H] = pencil_kernel<T, NX, CW, PENCIL_H>;
         o->fn[PENCIL_H_LAST] = pencil_kernel<T, NX, CW, PENCIL_H_LAST>;
         o->fn[PENCIL_INIT_W] = pencil_kernel<T, NX, CW, PENCIL_INIT_W>;
+        o->fn[PENCIL_HA] = pencil_kernel<T, NX, CW, PENCIL_HA>;
+        o->fn[PENCIL_HA_LAST] = pencil_kernel<T, NX, CW, PENCIL_HA_LAST>;
     } else {
         o->fn[PENCIL_H] = o->fn[PENCIL_H_LAST] = o->fn[PENCIL_INIT_W] = nullptr;
+        o->fn[PENCIL_HA] = o->fn[PENCIL_HA_LAST] = nullptr;
     }
     o->nt = C::NT;
     o->smem = C::SMEM;

@@ -656,8 +656,12 @@ enum PencilMode : int {
     PENCIL_H = 2,       // forward x, times h, store q, inverse x
     PENCIL_H_LAST = 3,  // forward x, times h, store q
     PENCIL_INIT_W = 4,  // h = exp(-w/N) from the fields, store it, inverse x
+    // the same with the concentration sums accumulated in the chain (second
+    // half of the chain: the new slot's partner slot is already stored)
+    PENCIL_HA = 5,       // forward x, times h, add the two phi products, inverse x (q not stored)
+    PENCIL_HA_LAST = 6,  // forward x, times h, store q_N (for Q), add the two phi products
 };
-constexpr int kPencilModes = 5;
+constexpr int kPencilModes = 7;
 
 template <typename T>
 struct PencilArgs {
@@ -675,6 +679,13 @@ struct PencilArgs {
     int hsel0, hsel1;         // h half used by chain 1 / chain 2 (0 = hA, 1 = hB)
     long long M;
     double Nd;                // N as a double (h = exp(-w/N))
+    // PENCIL_HA, PENCIL_HA_LAST: the new slot i+1 = (q_{i+1}, q^_{N-i}) and its
+    // partner slot N-i = (q_{N-i}, q^_{i+1}) give q_{i+1} q^_{i+1} and
+    // q_{N-i} q^_{N-i}, added into acc = (sum over A monomers, sum over B)
+    const T *partner;         // partner slot pairs (null: the slot pairs with itself, odd N)
+    T *acc;                   // (A, B) sums per mesh point
+    int acc_init;             // first accumulating step: acc starts at zero
+    int a_is_A, b_is_A;       // monomer i+1 / N-i is an A monomer (index <= NA)
 };
 
 template <typename T, int NX, int CW>
@@ -774,7 +785,43 @@ __device__ __forceinline__ void pencil_body(const PencilArgs<T> &a, const int ti
                 v[k2] = {va, vb};
             }
         }
-        if constexpr (MODE == PENCIL_H || MODE == PENCIL_INIT_W) {
+        if constexpr (MODE == PENCIL_HA || MODE == PENCIL_HA_LAST) {
+            static_assert(sizeof(T) == sizeof(float), "FP32 packed field only");
+            const int hs0 = a.hsel0, hs1 = a.hsel1;
+            float2 *accp = reinterpret_cast<float2 *>(a.acc);
+            const float2 *pp = reinterpret_cast<const float2 *>(a.partner);
+#pragma unroll
+            for (int k2 = 0; k2 < R2; k2++) {
+                const long long o = (long long)(k1 + R1 * k2) * ncol + col;
+                const float2 h = __ldg(reinterpret_cast<const float2 *>(a.h) + o);
+                const float va = v[k2].x * (hs0 ? h.y : h.x);
+                const float vb = v[k2].y * (hs1 ? h.y : h.x);
+                if (MODE == PENCIL_HA_LAST) __stcs(reinterpret_cast<float2 *>(a.qout) + o, make_float2(va, vb));
+                v[k2] = {va, vb};
+                // q_{i+1} q^_{i+1} = va * partner.y and q_{N-i} q^_{N-i} = partner.x * vb;
+                // with no partner (the middle slot of an odd chain) the slot
+                // is (q_m, q^_m) and gives the one product va * vb
+                float pa, pb = 0.f;
+                if (pp) {
+                    const float2 p = __ldcs(pp + o);
+                    pa = va * p.y;
+                    pb = p.x * vb;
+                } else {
+                    pa = va * vb;
+                }
+                float2 s = a.acc_init ? make_float2(0.f, 0.f) : accp[o];
+                if (a.a_is_A)
+                    s.x += pa;
+                else
+                    s.y += pa;
+                if (a.b_is_A)
+                    s.x += pb;
+                else
+                    s.y += pb;
+                accp[o] = s;
+            }
+        }
+        if constexpr (MODE == PENCIL_H || MODE == PENCIL_INIT_W || MODE == PENCIL_HA) {
             Dft<R2, 1, T>::run(v);
 #pragma unroll
             for (int u = 0; u < R2; u++) Tl[C::row(R2 * k1 + u) * CW + cl] = ctw<1>(v[u], twx[(u * k1) % NX]);
@@ -794,7 +841,7 @@ __device__ __forceinline__ void pencil_body(const PencilArgs<T> &a, const int ti
             }
         }
     }
-    if (MODE == PENCIL_POWER || MODE == PENCIL_H_LAST) return;
+    if (MODE == PENCIL_POWER || MODE == PENCIL_H_LAST || MODE == PENCIL_HA_LAST) return;
     __syncthreads();
 
     // X3: inverse stage A (strided) -> natural order, to global

@@ -214,6 +214,74 @@ __device__ __forceinline__ void concentrations_body(
     }
 }
 
+// The same with the sums over the monomers already formed by the contour chain
+// (the x-pencil's PENCIL_HA modes, FP32 packed path): acc[r] = (sum over A
+// monomers of q_i q^_i, sum over B monomers), h = slot 1 = (hA, hB).  Two mesh
+// points per thread and iteration; the dot-product partition is fixed by
+// (blk, nblk) as in concentrations_body.
+__device__ __forceinline__ void concentrations_acc_body(
+    const float *__restrict__ acc, const float *__restrict__ h, long long M, int N, double *__restrict__ phim,
+    double *__restrict__ phip, const double *__restrict__ Qd, float *__restrict__ Dh0, int nh, const HistPtrs &hist,
+    double *__restrict__ partials, const int blk, const int nblk)
+{
+    __shared__ double sh[kRedThreads / 32];
+    const double NQ = __dmul_rn((double)N, Qd[0]);
+    double dots[kRedWidth];
+#pragma unroll
+    for (int m = 0; m < kRedWidth; m++) dots[m] = 0.0;
+    const long long npair = M / 2;
+    const long long stride = (long long)nblk * blockDim.x;
+    for (long long g = (long long)blk * blockDim.x + threadIdx.x; g < npair; g += stride) {
+        const long long r0 = 2 * g;
+        const float4 s = *reinterpret_cast<const float4 *>(acc + 2 * r0);
+        const float4 hh = *reinterpret_cast<const float4 *>(h + 2 * r0);
+        const double sA[2] = {(double)s.x, (double)s.z}, sB[2] = {(double)s.y, (double)s.w};
+        const double hA[2] = {(double)hh.x, (double)hh.z}, hB[2] = {(double)hh.y, (double)hh.w};
+        double pm[2], pp[2];
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const double fA = sA[j] / __dmul_rn(NQ, hA[j]);
+            const double fB = sB[j] / __dmul_rn(NQ, hB[j]);
+            pm[j] = __dsub_rn(fA, fB);
+            pp[j] = __dadd_rn(fA, fB);
+        }
+        *reinterpret_cast<double2 *>(phim + r0) = make_double2(pm[0], pm[1]);
+        *reinterpret_cast<double2 *>(phip + r0) = make_double2(pp[0], pp[1]);
+        if (Dh0) {
+            double d[2];
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                d[j] = __dsub_rn(pp[j], 1.0);
+                dots[0] = __dadd_rn(dots[0], __dmul_rn(d[j], d[j]));
+            }
+            *reinterpret_cast<float2 *>(Dh0 + r0) = make_float2((float)d[0], (float)d[1]);
+#pragma unroll
+            for (int m = 1; m < kRedWidth; m++) {
+                if (m <= nh) {
+                    const float2 hv = *reinterpret_cast<const float2 *>(static_cast<const float *>(hist.p[m - 1]) + r0);
+                    dots[m] = __dadd_rn(dots[m], __dmul_rn(d[0], (double)hv.x));
+                    dots[m] = __dadd_rn(dots[m], __dmul_rn(d[1], (double)hv.y));
+                }
+            }
+        }
+    }
+    if (!Dh0) return;
+#pragma unroll
+    for (int m = 0; m < kRedWidth; m++) {
+        if (m > nh) break;
+        const double s = block_sum(dots[m], sh);
+        if (threadIdx.x == 0) partials[(long long)blk * kRedWidth + m] = s;
+    }
+}
+
+static __global__ void __launch_bounds__(kRedThreads, 4) concentrations_acc_kernel(
+    const float *__restrict__ acc, const float *__restrict__ h, long long M, int N, double *__restrict__ phim,
+    double *__restrict__ phip, const double *__restrict__ Qd, float *__restrict__ Dh0, int nh, HistPtrs hist,
+    double *__restrict__ partials)
+{
+    concentrations_acc_body(acc, h, M, N, phim, phip, Qd, Dh0, nh, hist, partials, blockIdx.x, gridDim.x);
+}
+
 template <typename T>
 static __global__ void __launch_bounds__(kRedThreads, 4) concentrations_kernel(
     const T *__restrict__ q, long long M, int N, int NA, const double *__restrict__ w,

@@ -312,13 +312,32 @@ void enqueue_chain_launches(lfts_ctx *c)
             PencilArgs<T> pi = pa;
             pi.qout = q;  // slot 1 = (hA, hB)
             launch_pencil<T>(c, PENCIL_INIT_W, pi, 2);
+            // With phi in the chain, the concentration sums are formed as the
+            // slots are made: slot i+1 = (q_{i+1}, q^_{N-i}) pairs with slot
+            // N-i = (q_{N-i}, q^_{i+1}).  From the middle of the chain on that
+            // partner is already stored, so the pencil adds the two products
+            // into acc and slot i+1 need not be stored (except slot N, for Q);
+            // the middle slot of an odd chain pairs with itself.
+            const bool acc = c->phi_in_chain;
+            bool first_acc = true;
             for (int i = 1; i < c->N; i++) {
                 launch_plane<T>(c, PLANE_G, a, 2);
                 PencilArgs<T> ph = pa;
                 ph.qout = q + (long long)i * 2 * M;  // slot i+1
                 ph.hsel0 = hsel_chain0(c, i);
                 ph.hsel1 = hsel_chain1(c, i);
-                launch_pencil<T>(c, i + 1 < c->N ? PENCIL_H : PENCIL_H_LAST, ph, 2);
+                const int p = c->N - i;  // partner slot
+                if (!acc || p > i + 1) {
+                    launch_pencil<T>(c, i + 1 < c->N ? PENCIL_H : PENCIL_H_LAST, ph, 2);
+                    continue;
+                }
+                ph.partner = p < i + 1 ? q + (long long)(p - 1) * 2 * M : nullptr;
+                ph.acc = static_cast<T *>(c->acc);
+                ph.acc_init = first_acc ? 1 : 0;
+                ph.a_is_A = i + 1 <= c->NA;
+                ph.b_is_A = p <= c->NA;
+                first_acc = false;
+                launch_pencil<T>(c, i + 1 < c->N ? PENCIL_HA : PENCIL_HA_LAST, ph, 2);
             }
             plane_q_sums_kernel<<<c->mx, 256, 0, c->st>>>(
                 reinterpret_cast<const float2 *>(q + (long long)(c->N - 1) * 2 * M), (long long)c->my * c->mz,
@@ -378,9 +397,14 @@ template <typename T>
 void enqueue_concs(lfts_ctx *c, void *Dh0, int nh, const HistPtrs &hist)
 {
     enqueue_chain<T>(c);
-    concentrations_kernel<T><<<stream_grid(c), kRedThreads, 0, c->st>>>(
-        static_cast<const T *>(c->q), c->M, c->N, c->NA, c->w, c->w + 2 * c->M, c->w + 3 * c->M, c->Qd,
-        static_cast<T *>(Dh0), nh, hist, c->partials);
+    if (c->phi_in_chain)
+        concentrations_acc_kernel<<<stream_grid(c), kRedThreads, 0, c->st>>>(
+            static_cast<const float *>(c->acc), static_cast<const float *>(c->q), c->M, c->N, c->w + 2 * c->M,
+            c->w + 3 * c->M, c->Qd, static_cast<float *>(Dh0), nh, hist, c->partials);
+    else
+        concentrations_kernel<T><<<stream_grid(c), kRedThreads, 0, c->st>>>(
+            static_cast<const T *>(c->q), c->M, c->N, c->NA, c->w, c->w + 2 * c->M, c->w + 3 * c->M, c->Qd,
+            static_cast<T *>(Dh0), nh, hist, c->partials);
     c->launches++;
     if (Dh0) {
         reduce_partials_kernel<<<1, 256, 0, c->st>>>(c->partials, c->red_blocks, nh + 1, c->red);
@@ -454,14 +478,15 @@ int apply_tiles(lfts_ctx *c, const lfts_tiles &t)
 {
     if (t.pencil_cw != 8 && t.pencil_cw != 16 && t.pencil_cw != 32) return LFTS_ERR_ARG;
     if (c->prec == LFTS_FP64) {
-        if (t.plane_stages != 2 || t.h_in_pencil != 0 || (t.two_streams != 0 && t.two_streams != 1))
+        if (t.plane_stages != 2 || t.h_in_pencil != 0 || (t.two_streams != 0 && t.two_streams != 1) ||
+            t.phi_in_chain != 0)
             return LFTS_ERR_ARG;
         int rc = set_pencil<double>(c, t.pencil_cw);
         if (rc) return rc;
         c->two_streams = t.two_streams == 1;
     } else {
         if ((t.plane_stages != 2 && t.plane_stages != 3) || (t.h_in_pencil != 0 && t.h_in_pencil != 1) ||
-            t.two_streams != 0)
+            t.two_streams != 0 || (t.phi_in_chain != 0 && t.phi_in_chain != 1) || (t.phi_in_chain && !t.h_in_pencil))
             return LFTS_ERR_ARG;
         PlaneKernels<float> pl{};
         const bool ok = t.plane_stages == 3 ? plane3_kernels(c->my, c->mz, &pl) : plane_c_kernels(c->my, c->mz, &pl);
@@ -469,6 +494,17 @@ int apply_tiles(lfts_ctx *c, const lfts_tiles &t)
         PencilKernels<float> pk{};
         if (!pencil_kernels(c->mx, t.pencil_cw, &pk)) return LFTS_ERR_UNSUPPORTED;
         if (t.h_in_pencil && !(pl.fn[PLANE_G] && pk.fn[PENCIL_H])) return LFTS_ERR_UNSUPPORTED;
+        if (t.phi_in_chain && !(pk.fn[PENCIL_HA] && pk.fn[PENCIL_HA_LAST])) return LFTS_ERR_UNSUPPORTED;
+        if (t.phi_in_chain && !c->acc) {
+            // the (A, B) concentration sums, FP32 pairs per mesh point
+            cudaError_t e = cudaMalloc(&c->acc, sizeof(float) * 2 * (size_t)c->M);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                c->acc = nullptr;
+                g_last_error = "device allocation of the concentration sums failed";
+                return LFTS_ERR_NOMEM;
+            }
+        }
         for (int m = 0; m < kPlaneModes; m++)
             if (pl.fn[m]) CK(cudaFuncSetAttribute(pl.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
         int rc = set_pencil<float>(c, t.pencil_cw);
@@ -476,6 +512,7 @@ int apply_tiles(lfts_ctx *c, const lfts_tiles &t)
         c->pl32 = pl;
         c->plane_stages = t.plane_stages;
         c->xh_chain = t.h_in_pencil == 1;
+        c->phi_in_chain = t.phi_in_chain == 1;
     }
     drop_chain_graph(c);
     return LFTS_OK;
@@ -489,24 +526,27 @@ lfts_tiles current_tiles(const lfts_ctx *c)
     t.plane_stages = fp64 ? 2 : c->plane_stages;
     t.h_in_pencil = (!fp64 && c->xh_chain) ? 1 : 0;
     t.two_streams = (fp64 && c->two_streams) ? 1 : 0;
+    t.phi_in_chain = (!fp64 && c->phi_in_chain) ? 1 : 0;
     return t;
 }
 
 // every valid combination for this context, restricted by the environment
-// (LFTS_PENCIL_CW, LFTS_XH_CHAIN, LFTS_ONE_STREAM fix one choice each)
+// (LFTS_PENCIL_CW, LFTS_XH_CHAIN, LFTS_ONE_STREAM, LFTS_PHI_IN_CHAIN fix one
+// choice each)
 std::vector<lfts_tiles> tile_candidates(const lfts_ctx *c)
 {
     std::vector<lfts_tiles> out;
     const char *fcw = std::getenv("LFTS_PENCIL_CW");
     const char *fxh = std::getenv("LFTS_XH_CHAIN");
     const char *fone = std::getenv("LFTS_ONE_STREAM");
+    const char *fphi = std::getenv("LFTS_PHI_IN_CHAIN");
     const int cw_forced = fcw ? std::atoi(fcw) : 0;
     for (int cw : {8, 16, 32}) {
         if (cw_forced > 0 && cw != cw_forced) continue;
         if (c->prec == LFTS_FP64) {
             for (int two : {1, 0}) {
                 if (fone && ((fone[0] == '1') == (two == 1))) continue;
-                out.push_back({cw, 2, 0, two});
+                out.push_back({cw, 2, 0, two, 0});
             }
             continue;
         }
@@ -514,12 +554,17 @@ std::vector<lfts_tiles> tile_candidates(const lfts_ctx *c)
         PencilKernels<float> pk{};
         const bool has3 = plane3_kernels(c->my, c->mz, &p3);
         const bool hasx = has3 && p3.fn[PLANE_G] && pencil_kernels(c->mx, cw, &pk) && pk.fn[PENCIL_H];
+        const bool hasa = hasx && pk.fn[PENCIL_HA] && pk.fn[PENCIL_HA_LAST];
         for (int st : {3, 2}) {
             if (st == 3 && !has3) continue;
             for (int xh : {1, 0}) {
                 if (xh && (st != 3 || !hasx)) continue;
                 if (fxh && ((fxh[0] != '0') != (xh == 1))) continue;
-                out.push_back({cw, st, xh, 0});
+                for (int phi : {0, 1}) {
+                    if (phi && (!xh || !hasa)) continue;
+                    if (fphi && ((fphi[0] != '0') != (phi == 1))) continue;
+                    out.push_back({cw, st, xh, 0, phi});
+                }
             }
         }
     }
@@ -534,15 +579,33 @@ lfts_tiles default_tiles(const lfts_ctx *c)
     const int cw = c->prec == LFTS_FP64 ? kDefaultCwFp64 : kDefaultCwFp32;
     for (const lfts_tiles &t : cand)
         if (t.pencil_cw == cw) return t;  // candidates come best-guess first
-    return cand.empty() ? lfts_tiles{cw, 2, 0, c->prec == LFTS_FP64 ? 1 : 0} : cand.front();
+    return cand.empty() ? lfts_tiles{cw, 2, 0, c->prec == LFTS_FP64 ? 1 : 0, 0} : cand.front();
 }
 
+// one calc_concs without the Anderson dot products: the chain, then the
+// concentrations from the stored slots or from the sums the chain formed
+template <typename T>
+void enqueue_calc(lfts_ctx *c)
+{
+    enqueue_chain_launches<T>(c);
+    if (c->phi_in_chain)
+        concentrations_acc_kernel<<<stream_grid(c), kRedThreads, 0, c->st>>>(
+            static_cast<const float *>(c->acc), static_cast<const float *>(c->q), c->M, c->N, c->w + 2 * c->M,
+            c->w + 3 * c->M, c->Qd, nullptr, 0, HistPtrs{}, c->partials);
+    else
+        concentrations_kernel<T><<<stream_grid(c), kRedThreads, 0, c->st>>>(
+            static_cast<const T *>(c->q), c->M, c->N, c->NA, c->w, c->w + 2 * c->M, c->w + 3 * c->M, c->Qd, nullptr,
+            0, HistPtrs{}, c->partials);
+}
+
+// a tile choice is timed on whole calc_concs (chain + concentrations): the
+// choices differ in how the concentration work is split between them
 template <typename T>
 int time_chain(lfts_ctx *c, cudaEvent_t e0, cudaEvent_t e1, float *ms)
 {
-    enqueue_chain_launches<T>(c);  // warm-up
+    enqueue_calc<T>(c);  // warm-up
     CK(cudaEventRecord(e0, c->st));
-    for (int r = 0; r < 3; r++) enqueue_chain_launches<T>(c);
+    for (int r = 0; r < 3; r++) enqueue_calc<T>(c);
     CK(cudaEventRecord(e1, c->st));
     CK(cudaEventSynchronize(e1));
     CK(cudaGetLastError());
@@ -827,8 +890,12 @@ int capture_mix_graph(lfts_ctx *c, cudaGraph_t *g_out)
     if (e != cudaSuccess) return fail(e, "mix graph body capture");
     const long long launches0 = c->launches;
     enqueue_chain_launches<T>(c);
-    mix_conc_kernel<T><<<stream_grid(c), kRedThreads, 0, c->st>>>(S, static_cast<const T *>(c->q), c->N, c->NA,
-                                                                    c->Qd);
+    if (c->phi_in_chain)
+        mix_conc_acc_kernel<<<stream_grid(c), kRedThreads, 0, c->st>>>(S, static_cast<const float *>(c->acc),
+                                                                        static_cast<const float *>(c->q), c->N, c->Qd);
+    else
+        mix_conc_kernel<T><<<stream_grid(c), kRedThreads, 0, c->st>>>(S, static_cast<const T *>(c->q), c->N, c->NA,
+                                                                        c->Qd);
     mix_solve_kernel<<<1, 256, 0, c->st>>>(S);
     mix_update_kernel<T><<<stream_grid(c), 256, 0, c->st>>>(S);
     mix_control_kernel<<<1, 32, 0, c->st>>>(S, loop);
@@ -1075,6 +1142,7 @@ void ctx_free(lfts_ctx *c)
     cudaFree(c->adj_partial);
     cudaFree(c->adj_buf);
     drop_chain_graph(c);
+    cudaFree(c->acc);
     cudaFree(c->d_mix);
     cudaFree(c->d_lambda);
     if (c->st1) cudaStreamSynchronize(c->st1);
@@ -1356,6 +1424,7 @@ int lfts_device_bytes(const lfts_ctx *c, size_t *bytes)
     size_t b = 4 * M * 8 + c->tsize * 2 * M * c->N + c->tsize * 4 * (size_t)c->mx * c->my * c->KZ;
     b += 2 * M * 8 + 2 * kRedWidth * M * c->tsize + c->Mk * 8;
     if (c->sk_own_spec) b += c->Mk * 16;
+    if (c->acc) b += 8 * M;
     *bytes = b;
     return LFTS_OK;
 }
@@ -1678,6 +1747,10 @@ int lfts_profile_iteration(lfts_ctx *c, int reps, double *ms_chain, double *ms_c
             concentrations_kernel<double><<<stream_grid(c), kRedThreads, 0, c->st>>>(
                 static_cast<const double *>(c->q), M, c->N, c->NA, c->w, c->w + 2 * M, c->w + 3 * M, c->Qd,
                 static_cast<double *>(c->Dh[c->cur]), kMaxHist, Dhp, c->partials);
+        else if (c->phi_in_chain)
+            concentrations_acc_kernel<<<stream_grid(c), kRedThreads, 0, c->st>>>(
+                static_cast<const float *>(c->acc), static_cast<const float *>(c->q), M, c->N, c->w + 2 * M,
+                c->w + 3 * M, c->Qd, static_cast<float *>(c->Dh[c->cur]), kMaxHist, Dhp, c->partials);
         else
             concentrations_kernel<float><<<stream_grid(c), kRedThreads, 0, c->st>>>(
                 static_cast<const float *>(c->q), M, c->N, c->NA, c->w, c->w + 2 * M, c->w + 3 * M, c->Qd,
@@ -1758,6 +1831,14 @@ int lfts_get_propagators(lfts_ctx *c, double *q_host)
         CK(cudaMemcpyAsync(q_host + 2 * c->M, c->q, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
         CK(cudaStreamSynchronize(c->st));
     } else {
+        if (c->phi_in_chain && c->fields_set) {
+            // the chain that forms the concentration sums leaves the later slots
+            // unstored: run the storing chain on the same fields
+            c->phi_in_chain = false;
+            enqueue_chain_launches<float>(c);
+            c->phi_in_chain = true;
+            CK(cudaGetLastError());
+        }
         // FP32 slots hold (q_i, q^_{N+1-i}) pairs: back to the [q_i | q^] halves
         std::vector<float> tmp(n);
         CK(cudaMemcpyAsync(tmp.data(), c->q, sizeof(float) * n, cudaMemcpyDeviceToHost, c->st));

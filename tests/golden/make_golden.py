@@ -140,17 +140,39 @@ def case_config(name, hdr, n_steps, stride, field_seed=None, sample_every=1, sen
     w[:2 * M] = start
     out["cc_lnQ"] = sys_.calc_concs(w)
     out.update(_compact("cc_w", w, M, stride))
+    sys_.close()
     if sensitivity:
-        ks = []
+        # the reference's own reproducibility: the same run (initial mix, the
+        # same Langevin steps and noise) from the start and from the start
+        # times (1 + 1e-15); how far its fields, ln Q and H move is the
+        # tolerance a faithful restatement can be held to on this run
+        from pyoracle import RefLangevin
+        sigma = float(np.sqrt(2.0 * M * dt / (C * np.prod(L))))
+        runs = []
         for eps in (0.0, 1e-15):
+            s2 = RefSys(NA, N - NA, m, L)
+            lg = RefLangevin(123456789, sigma, M)
             wp = np.zeros(4 * M)
             wp[:2 * M] = start * (1.0 + eps)
-            ks.append(sys_.mix(wp))
-            sys_.close()
-            sys_ = RefSys(NA, N - NA, m, L)
-        out["mix_K_unperturbed"], out["mix_K_perturbed"] = ks
-        print(name, "mix K with and without a 1e-15 perturbation", ks)
-    sys_.close()
+            k0 = s2.mix(wp)
+            w0 = wp.copy()
+            ks, lqs = [k0], []
+            for _ in range(n_steps):
+                k, lq = lg.full_step(s2, wp, XN, dt)
+                ks.append(k)
+                lqs.append(lq)
+            lnq_end = s2.calc_concs(wp)
+            H = -lnq_end + (np.sum(wp[:M] ** 2) / XN - np.sum(wp[M:2 * M])) / M
+            runs.append((ks, w0, wp.copy(), np.array(lqs), H))
+            s2.close()
+            lg.close()
+        (ka, w0a, wea, lqa, Ha), (kb, w0b, web, lqb, Hb) = runs
+        quarter_diff = lambda a, b: np.abs(a - b).reshape(4, M).max(axis=1)  # noqa: E731
+        out.update(mix_K_unperturbed=ka[0], mix_K_perturbed=kb[0], K_perturbed=np.array(kb[1:]),
+                   spread_w0=quarter_diff(w0a, w0b), spread_w_end=quarter_diff(wea, web),
+                   spread_lnQ=np.abs(lqa - lqb), spread_H=abs(Ha - Hb))
+        print(name, "K with and without a 1e-15 perturbation", ka, kb, "spread w0", out["spread_w0"],
+              "spread H", out["spread_H"])
     work = tempfile.mkdtemp()
     cwd = os.getcwd()
     try:

@@ -13,9 +13,11 @@ per-quarter sums):
 
 Per call (calc_concs of the start fields) the FP64 path is held to 1e-10 and
 FP32-mixed to 1e-5 on phi.  Over trajectories the FP64 path is held to 1e-10
-on ln Q with the Anderson counts equal -- unless the fixture records that the
-reference's own mix changes its count under a 1e-15 perturbation of the start
-(roundoff-sensitive), in which case the run is held to the mixing tolerance."""
+on ln Q with the Anderson counts equal, or, where the reference itself is not
+that reproducible, to 20 times how far the reference's own run moves when its
+start is perturbed by 1e-15 (the fixture records that run: at 32^3 its mixed
+w+ moves by 2e-7 relative with the same counts; the 64^3 lamellar starts
+change their Anderson counts)."""
 import numpy as np
 import pytest
 
@@ -33,20 +35,32 @@ def lfts(native_lib):
     return lfts_cpu_b200
 
 
-def check_compact(w, g, prefix, tol, quarters=(0, 1, 2, 3)):
-    """w (4M) against the fixture's strided values and per-quarter sums."""
+SPREAD_FACTOR = 20.0  # times the reference's own change under a 1e-15 perturbation of the start
+
+
+def check_compact(w, g, prefix, tol, quarters=(0, 1, 2, 3), spread=None):
+    """w (4M) against the fixture's strided values and per-quarter sums.
+    Errors are relative to the quarter's largest value (to the larger of
+    phi- and phi+ for the two phi quarters).  With `spread` (per-quarter
+    absolute change of the reference's own run under a 1e-15 perturbation of
+    its start) the tolerance is at least SPREAD_FACTOR times that."""
     M = len(w) // 4
     stride = int(g["stride"])
     s_ref = g[prefix + "_s"]
     idx = np.arange(0, 4 * M, stride)
+    sel = [(idx >= q * M) & (idx < (q + 1) * M) for q in range(4)]
     for qtr in quarters:
-        sel = (idx >= qtr * M) & (idx < (qtr + 1) * M)
-        a, b = w[::stride][sel], s_ref[sel]
-        assert rel_err(a, b) < tol, (prefix, qtr, rel_err(a, b))
+        a, b = w[::stride][sel[qtr]], s_ref[sel[qtr]]
+        scale = np.max(np.abs(b))
+        if qtr >= 2:
+            scale = max(np.max(np.abs(s_ref[sel[2]])), np.max(np.abs(s_ref[sel[3]])))
+        scale = max(scale, 1e-300)
+        t = tol if spread is None else max(tol, SPREAD_FACTOR * float(spread[qtr]) / scale)
+        err = float(np.max(np.abs(a - b))) / scale
+        assert err < t, (prefix, qtr, err, t)
         q = w[qtr * M:(qtr + 1) * M]
-        scale = max(np.max(np.abs(b)), 1e-300)
-        assert abs(q.sum() - g[prefix + "_sum"][qtr]) <= tol * scale * M, (prefix, qtr)
-        assert abs((q * q).sum() - g[prefix + "_sq"][qtr]) <= 2 * tol * scale * scale * M, (prefix, qtr)
+        assert abs(q.sum() - g[prefix + "_sum"][qtr]) <= t * scale * M, (prefix, qtr)
+        assert abs((q * q).sum() - g[prefix + "_sq"][qtr]) <= 2 * t * scale * scale * M, (prefix, qtr)
 
 
 def start_fields(lfts, g, hdr, M):
@@ -67,7 +81,10 @@ def setup(lfts, name, precision=0):
 
 
 def sensitive(g):
-    return int(g["mix_K_unperturbed"]) != int(g["mix_K_perturbed"])
+    """The reference's own Anderson counts change under a 1e-15 perturbation
+    of the start (initial mix or any step)."""
+    return (int(g["mix_K_unperturbed"]) != int(g["mix_K_perturbed"])
+            or list(g["K_perturbed"]) != list(g["K"]))
 
 
 @pytest.mark.parametrize("name", ["cfg1_32", "cfg2_64", "cfg4_64"])
@@ -80,7 +97,7 @@ def test_config_calc_concs_of_the_start(lfts, name, precision):
     w = s.get_fields()
     tol = FP64_TOL if precision == 0 else 1e-5
     assert abs(lnQ - float(g["cc_lnQ"])) < tol * max(1.0, abs(float(g["cc_lnQ"])))
-    check_compact(w, g, "cc_w", tol, quarters=(2, 3))
+    check_compact(w, g, "cc_w", tol, quarters=(2, 3))  # phi relative to its largest value
     s.close()
 
 
@@ -104,33 +121,36 @@ def run_trajectory(lfts, g, hdr, M, s):
 @pytest.mark.parametrize("name", ["cfg1_32", "cfg2_64", "cfg4_64"])
 def test_config_trajectory_fp64(lfts, name):
     """Initial mix and Langevin steps with the reference's noise stream: the
-    mixed start, K per step, ln Q per step, fields, S(k) and its binned text, H."""
+    mixed start, K per step, ln Q per step, fields, S(k) and its binned text,
+    H.  Each is held to the FP64 bar (1e-10 on ln Q, 1e-9 .. 1e-8 on fields)
+    or to SPREAD_FACTOR times how far the reference's own run moves when its
+    start is perturbed by 1e-15, whichever is looser; the Anderson counts
+    must be equal wherever the reference's own counts are reproducible."""
     g, hdr, M, s = setup(lfts, name)
     w0, Ks, lnQs = run_trajectory(lfts, g, hdr, M, s)
-    if sensitive(g):
-        # converged to the same saddle point within the mixing tolerance (1e-4)
-        check_compact(w0, g, "w0", 1e-3, quarters=(0, 1))
-        assert np.max(np.abs(lnQs - g["lnQ"])) < 1e-4
-        check_compact(s.get_fields(), g, "w_end", 1e-3, quarters=(0,))
-        assert abs(s.get_H() - float(g["H"])) < 1e-4
-        s.close()
-        return
-    check_compact(w0, g, "w0", 1e-9)
-    assert Ks == list(g["K"])
-    assert np.max(np.abs(lnQs - g["lnQ"])) < FP64_TOL * max(1.0, np.max(np.abs(g["lnQ"])))
-    check_compact(s.get_fields(), g, "w_end", 1e-8)
+    check_compact(w0, g, "w0", 1e-9, spread=g["spread_w0"])
+    if not sensitive(g):
+        assert Ks == list(g["K"])
+    lnq_tol = np.maximum(FP64_TOL * max(1.0, np.max(np.abs(g["lnQ"]))), SPREAD_FACTOR * g["spread_lnQ"])
+    assert np.all(np.abs(lnQs - g["lnQ"]) < lnq_tol), (lnQs - g["lnQ"], lnq_tol)
+    w = s.get_fields()
+    check_compact(w, g, "w_end", 1e-8, spread=g["spread_w_end"])
+    stride = int(g["stride"])
     S, ns = s.sk_get()
     assert ns == int(g["nsamples"])
-    stride = int(g["stride"])
-    assert rel_err(S[::stride], g["S_s"]) < 1e-8
-    assert abs(S.sum() - float(g["S_sum"])) < 1e-8 * abs(float(g["S_sum"]))
+    # S(k) = |FFT(W-)|^2 summed over the samples: its error follows W-'s
+    sw = float(np.max(np.abs(g["w_end_s"][: (M + stride - 1) // stride])))
+    s_tol = max(1e-8, 2 * SPREAD_FACTOR * float(g["spread_w_end"][0]) / sw)
+    assert rel_err(S[::stride], g["S_s"]) < s_tol
+    assert abs(S.sum() - float(g["S_sum"])) < s_tol * abs(float(g["S_sum"]))
     K, Sb = s.sk_bin(1e-5)
     ref = np.array([[float(v) for v in ln.split("\t")] for ln in str(g["struct_text"]).strip().split("\n")])
     assert len(K) == len(ref)
     assert np.max(np.abs(K - ref[:, 0])) < 1e-8
-    assert np.max(np.abs(Sb - ref[:, 1])) < 1e-6
-    assert abs(s.get_H() - float(g["H"])) < FP64_TOL * 10 * max(1.0, abs(float(g["H"])))
-    check_compact(s.get_fields(), g, "w_H", 1e-8)
+    assert np.max(np.abs(Sb - ref[:, 1])) < max(1e-6, s_tol * np.max(np.abs(ref[:, 1])))
+    h_tol = max(FP64_TOL * 10 * max(1.0, abs(float(g["H"]))), SPREAD_FACTOR * float(g["spread_H"]))
+    assert abs(s.get_H() - float(g["H"])) < h_tol
+    check_compact(s.get_fields(), g, "w_H", 1e-8, spread=g["spread_w_end"])
     s.close()
 
 

@@ -36,9 +36,11 @@ def make(lfts, host_loop, N, NA, m, precision, tiles=None):
 @pytest.mark.parametrize("precision,m,N,NA,tiles", [
     (0, (32, 32, 32), 16, 6, None),
     (1, (32, 32, 32), 16, 6, None),
-    (0, (24, 24, 24), 12, 12, None),
+    (0, (24, 24, 24), 12, 7, None),
+    (1, (24, 24, 24), 12, 1, None),
     (1, (128, 128, 128), 8, 3, dict(pencil_cw=16, plane_stages=3, h_in_pencil=1, two_streams=0)),
     (1, (128, 128, 128), 8, 5, dict(pencil_cw=16, plane_stages=3, h_in_pencil=0, two_streams=0)),
+    (1, (128, 128, 128), 7, 3, dict(pencil_cw=16, plane_stages=3, h_in_pencil=1, two_streams=0, phi_in_chain=1)),
 ])
 def test_device_loop_equals_host_loop(lfts, precision, m, N, NA, tiles):
     M = int(np.prod(m))

@@ -1,8 +1,9 @@
 """Tile choices of the contour chain and their autotuner: the x-pencil width
 and (FP64) the stream split are bitwise-neutral; every FP32-mixed choice
-(plane stages, where h is applied) agrees with the others and with FP64
-within the FP32-mixed tolerance; the autotuner's choice is a valid candidate;
-invalid choices are refused and leave the context as it was."""
+(plane stages, where h is applied, concentration sums formed in the chain)
+agrees with the others and with FP64 within the FP32-mixed tolerance; the
+autotuner's choice is a valid candidate; invalid choices are refused and
+leave the context as it was."""
 import itertools
 
 import numpy as np
@@ -24,12 +25,12 @@ def lfts(native_lib):
 def candidates(precision, m):
     """Every tile combination, valid or not, for the context to accept or refuse."""
     out = []
-    for cw, st, xh, two in itertools.product((8, 16, 32), (2, 3), (0, 1), (0, 1)):
-        if precision == 0 and (st != 2 or xh):
+    for cw, st, xh, two, phi in itertools.product((8, 16, 32), (2, 3), (0, 1), (0, 1), (0, 1)):
+        if precision == 0 and (st != 2 or xh or phi):
             continue
-        if precision == 1 and two:
+        if precision == 1 and (two or (phi and not xh)):
             continue
-        out.append(dict(pencil_cw=cw, plane_stages=st, h_in_pencil=xh, two_streams=two))
+        out.append(dict(pencil_cw=cw, plane_stages=st, h_in_pencil=xh, two_streams=two, phi_in_chain=phi))
     return out
 
 
@@ -91,7 +92,7 @@ def test_fp32_tiles_agree_within_tolerance(lfts, m, N, NA):
     # the pencil width alone changes no value
     by_rest = {}
     for t, lnq, phi in res:
-        key = (t["plane_stages"], t["h_in_pencil"])
+        key = (t["plane_stages"], t["h_in_pencil"], t["phi_in_chain"])
         if key in by_rest:
             assert lnq == by_rest[key][0] and np.array_equal(phi, by_rest[key][1]), t
         else:
@@ -106,3 +107,29 @@ def test_autotuned_choices_are_candidates(lfts):
         assert t in candidates(precision, m) and valid(precision, m, t), (m, t)
         assert s.tuning() == (t["pencil_cw"], t["plane_stages"])
         s.close()
+
+
+@pytest.mark.parametrize("N,NA", [(2, 1), (3, 1), (3, 2), (7, 3), (8, 8), (8, 0), (64, 25)])
+def test_phi_in_chain_matches_the_separate_pass(lfts, N, NA):
+    """Concentration sums formed in the x-pencil from the middle of the chain
+    on (each new slot times its stored partner; odd N: the middle slot with
+    itself; the last step pairs slot N with h) against the separate pass over
+    all stored slots: ln Q bitwise (both take Q from the stored slot N), phi to
+    the FP32-mixed tolerance, and the propagators bitwise (the storing chain
+    is rerun for them)."""
+    m = (128, 128, 128)
+    M = int(np.prod(m))
+    w2 = np.random.default_rng(N * 100 + NA).normal(0.0, 0.5, 2 * M)
+    s = lfts.System(N, NA, 16.0, 100.0, 0.5, m, (8.0, 8.0, 8.0), precision=1)
+    s.set_fields(w2)
+    out = []
+    for phi in (0, 1):
+        s.set_tiles(16, 3, 1, 0, phi)
+        lnq = s.calc_concs()
+        out.append((lnq, s.get_fields()[2 * M:], s.propagators() if N <= 8 else None))
+    (lq0, p0, q0), (lq1, p1, q1) = out
+    assert lq1 == lq0
+    assert rel_err(p1, p0) < FP32_PHI_TOL
+    if q0 is not None:
+        assert np.array_equal(q1, q0)
+    s.close()
