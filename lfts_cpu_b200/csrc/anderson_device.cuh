@@ -3,8 +3,8 @@
 // (ensemble_kernels.cuh) and a single context's device-side Anderson loop
 // (lfts_capi.cu): one block reduces the residual dot products in a fixed
 // order, one warp builds and solves the least-squares system and does the
-// history bookkeeping, so both produce bit for bit what the host loop
-// (anderson_mix in lfts_capi.cu) produces.
+// history bookkeeping, so both produce bit for bit what the host-driven loop
+// (anderson_mix_host in lfts_capi.cu) produces.
 #pragma once
 #include "field_kernels.cuh"
 
