@@ -334,6 +334,22 @@ def run_precision(lfts, precision, steps, warmup, rank, device, torch, clocks=No
     return res
 
 
+def time_calc_concs(s, torch, device, reps=5):
+    """Mean ms of one calc_concs (contour chain, Q, concentrations) on the
+    context's current fields: CUDA events on the context's stream around the
+    C-ABI call, after one warm call."""
+    stream = torch.cuda.ExternalStream(s.stream, device=f"cuda:{device}")
+    s.calc_concs()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(reps):
+        s.calc_concs()
+    ev1.record(stream)
+    ev1.synchronize()
+    return ev0.elapsed_time(ev1) / reps
+
+
 def ensemble_config(seed=2024, nrep=32):
     """The batched configuration: nrep replicas, meshes drawn from seed among
     32^3, 48^3, 64^3, 96^3, L = mesh/16, N=64, NA in [16,48], XN in [12,20],
@@ -374,7 +390,7 @@ def ensemble_bench(lfts, torch, device, steps=5, warmup=3):
            "mean_anderson_K": float(K.mean()),
            "mesh_point_contour_steps_per_s": point_steps * 1e3 / ms,
            "tiles": {str(d["m"][0]): e.tiles(r) for r, d in enumerate(reps)},
-           "timing": f"{steps} steps after {warmup} warm-up steps, one CUDA graph launch per step",
+           "timing": f"{steps} steps after {warmup} warm-up steps, the timed steps as one CUDA graph launch",
            "sequential_single_contexts_ms_per_step": seq_ms,
            "speedup_vs_sequential_single_contexts": seq_ms / ms}
     e.close()
@@ -565,6 +581,7 @@ def main(argv=None):
     # once-per-step kernels
     part_chain, part_conc, part_upd = fp32_sys.profile_iteration(5)
     tiles32 = fp32_sys.tiles()
+    ms_calc = time_calc_concs(fp32_sys, torch, device)
     fp32_sys.close()
     fp64 = run_precision(lfts, lfts.LFTS_FP64, args.steps, args.warmup, rank, device, torch, None)
     fp64.pop("system").close()
@@ -615,9 +632,20 @@ def main(argv=None):
             except Exception as e:  # reported, not fatal
                 ens = {"failed": str(e)}
         traffic = None
+        traffic_cc = None
         tp = os.path.join(ROOT, "profiles", "contour_step_traffic.json")
         if os.path.exists(tp):
-            traffic = json.load(open(tp)).get("bytes_per_step_fp32_128")
+            tj = json.load(open(tp))
+            traffic = tj.get("bytes_per_step_fp32_128")
+            traffic_cc = tj.get("bytes_per_calc_concs_fp32_128", {}).get("phi_in_chain" if tiles32.get(
+                "phi_in_chain") else "separate_pass")
+        # the roofline unit SURVEY-style: one calc_concs (the contour chain, Q
+        # and the concentrations), algorithmic bytes W_cc = 7 N M propagator
+        # words (FP32) + 6 M field words (FP64): read q, read h, write q per
+        # chain step, the N stored propagators read back for phi, w in, h and
+        # phi out -- wherever the work happens (with phi_in_chain the stored
+        # propagators are read inside the chain instead of by a later pass)
+        achieved_cc = W_cc_bytes / (ms_calc * 1e-3) / 1e9
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak",
@@ -628,11 +656,19 @@ def main(argv=None):
                     "d2h_bytes_per_step": fp32["d2h_bytes_per_step"],
                     "steps": "the timed steps replayed from the same state and noise, noise read from pinned host memory",
                     "same_anderson_K": fp32["e2e_same_K"]},
-            "roofline": {"bound": "hbm", "kernel": "contour step (yz-plane + x-pencil kernels, both chains, FP32)",
-                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_kind": peak_kind, "traffic": traffic,
-                         "algorithmic_bytes_per_launch": step_bytes, "ms_per_step": step_ms,
-                         "ms_plane_alone": pl, "ms_pencil_alone": pe},
+            "roofline": {"bound": "hbm", "kernel": "calc_concs: contour chain (yz-plane + x-pencil kernels, both "
+                                                   "chains, FP32) + Q + concentrations, one graph replay",
+                         "achieved": achieved_cc, "peak": peak, "unit": "GB/s", "frac": achieved_cc / peak,
+                         "peak_kind": peak_kind, "traffic": traffic_cc,
+                         "algorithmic_bytes_per_launch": W_cc_bytes, "ms_per_launch": ms_calc,
+                         "unit_of_work": "one calc_concs, W_cc = 7 N M propagator words (4 B) + 6 M field words (8 B)"},
+            "roofline_contour_step": {"bound": "hbm", "kernel": "one contour step (yz-plane + x-pencil kernels)",
+                                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                                      "peak_kind": peak_kind, "traffic": traffic,
+                                      "algorithmic_bytes_per_launch": step_bytes, "ms_per_step": step_ms,
+                                      "ms_plane_alone": pl, "ms_pencil_alone": pe,
+                                      "note": "with phi_in_chain the second half of the steps also reads the "
+                                              "partner slots and adds the concentration sums (not in these bytes)"},
             "cpu_baseline": cpu,
             "clocks": fp32["clocks"],
             "gpu_launches": fp32["launches"],

@@ -80,8 +80,9 @@ struct lfts_ctx {
     cudaGraphExec_t chain_exec = nullptr;
     long long chain_kernels = 0;  // kernels in one replay of chain_exec
     // the device-side Anderson loop (anderson_device.cuh): one graph launch per
-    // mix; LFTS_HOST_MIX=1 keeps the loop on the host
-    bool mix_on_device = true;
+    // mix, selected by LFTS_DEVICE_MIX=1 (measured slower than the host-driven
+    // loop on B200: each WHILE-node iteration costs more than a host round trip)
+    bool mix_on_device = false;
     int mix_graph_state = 0;  // 0 not built, 1 built, -1 building failed (host loop)
     void *d_mix = nullptr;    // MixState
     double *d_lambda = nullptr;

@@ -754,6 +754,21 @@ __device__ __forceinline__ void pencil_body(const PencilArgs<T> &a, const int ti
         const int cl = t % CW, k1 = t / CW, col = col0 + cl;
         if (col >= ncol) continue;
         cpx<T> v[R2];
+        // PENCIL_HA*: the partner slot (HBM) and the running sums (L2) of this
+        // task's points go out before its shared-memory reads and transform, so
+        // their latency overlaps that work instead of each point's update
+        constexpr bool kAcc = MODE == PENCIL_HA || MODE == PENCIL_HA_LAST;
+        float2 pv[kAcc ? R2 : 1], av[kAcc ? R2 : 1];
+        if constexpr (kAcc) {
+            const float2 *__restrict__ pp = reinterpret_cast<const float2 *>(a.partner);
+            const float2 *__restrict__ ap = reinterpret_cast<const float2 *>(a.acc);
+#pragma unroll
+            for (int k2 = 0; k2 < R2; k2++) {
+                const long long o = (long long)(k1 + R1 * k2) * ncol + col;
+                pv[k2] = pp ? __ldcs(pp + o) : make_float2(0.f, 0.f);
+                av[k2] = a.acc_init ? make_float2(0.f, 0.f) : ap[o];
+            }
+        }
         if constexpr (MODE == PENCIL_INIT_W) {
             // hA = exp(-(W- + w+)/N), hB = exp(-(-W- + w+)/N)  (src/diblock.cc:64-72),
             // single-precision exponential as the FP32 plane kernels' INIT_W
@@ -789,7 +804,7 @@ __device__ __forceinline__ void pencil_body(const PencilArgs<T> &a, const int ti
             static_assert(sizeof(T) == sizeof(float), "FP32 packed field only");
             const int hs0 = a.hsel0, hs1 = a.hsel1;
             float2 *accp = reinterpret_cast<float2 *>(a.acc);
-            const float2 *pp = reinterpret_cast<const float2 *>(a.partner);
+            const bool has_partner = a.partner != nullptr;
 #pragma unroll
             for (int k2 = 0; k2 < R2; k2++) {
                 const long long o = (long long)(k1 + R1 * k2) * ncol + col;
@@ -802,14 +817,13 @@ __device__ __forceinline__ void pencil_body(const PencilArgs<T> &a, const int ti
                 // with no partner (the middle slot of an odd chain) the slot
                 // is (q_m, q^_m) and gives the one product va * vb
                 float pa, pb = 0.f;
-                if (pp) {
-                    const float2 p = __ldcs(pp + o);
-                    pa = va * p.y;
-                    pb = p.x * vb;
+                if (has_partner) {
+                    pa = va * pv[k2].y;
+                    pb = pv[k2].x * vb;
                 } else {
                     pa = va * vb;
                 }
-                float2 s = a.acc_init ? make_float2(0.f, 0.f) : accp[o];
+                float2 s = av[k2];
                 if (a.a_is_A)
                     s.x += pa;
                 else

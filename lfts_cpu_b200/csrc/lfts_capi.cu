@@ -949,6 +949,10 @@ int ensure_mix_graph(lfts_ctx *c, int maxIter)
     }
     c->use_pdl = pdl;
     c->mix_graph_state = rc ? -1 : 1;
+    if (const char *v = getenv("LFTS_VERBOSE"))
+        if (v[0] == '1')
+            fprintf(stderr, "lfts: Anderson-loop graph %s%s\n", rc ? "not built: " : "built, chain ",
+                    rc ? g_last_error.c_str() : (c->mix_pdl ? "with programmatic edges" : "without programmatic edges"));
     return rc;
 }
 
@@ -1365,7 +1369,7 @@ int lfts_create(const lfts_params *p, int precision, int device, lfts_ctx **out)
     if (const char *e = getenv("LFTS_NO_PDL")) c->use_pdl = !(e[0] == '1');
     if (const char *e = getenv("LFTS_ONE_STREAM")) c->two_streams = !(e[0] == '1');
     if (const char *e = getenv("LFTS_NO_GRAPH")) c->use_graph = !(e[0] == '1');
-    if (const char *e = getenv("LFTS_HOST_MIX")) c->mix_on_device = !(e[0] == '1');
+    if (const char *e = getenv("LFTS_DEVICE_MIX")) c->mix_on_device = e[0] == '1';
     if (!c->use_graph) c->mix_on_device = false;
     int rc = LFTS_OK;
     auto fail = [&](int code) {

@@ -1,7 +1,7 @@
 """The Anderson loop of a single context on the device (one CUDA graph per
 mix: a WHILE node around the contour chain, the concentrations with the
 residual dot products, the least squares on one warp, the w+ update) against
-the host-driven loop (LFTS_HOST_MIX=1): the same Anderson counts and the same
+the host-driven loop (the default; LFTS_DEVICE_MIX=1 selects the device loop): the same Anderson counts and the same
 fields bit for bit, over an initial mix and Langevin steps, both precisions,
 both FP32 chain orders."""
 import os
@@ -19,15 +19,15 @@ def lfts(native_lib):
 
 
 def make(lfts, host_loop, N, NA, m, precision, tiles=None):
-    old = os.environ.get("LFTS_HOST_MIX")
-    os.environ["LFTS_HOST_MIX"] = "1" if host_loop else "0"
+    old = os.environ.get("LFTS_DEVICE_MIX")
+    os.environ["LFTS_DEVICE_MIX"] = "0" if host_loop else "1"
     try:
         s = lfts.System(N, NA, 15.0, 80.0, 0.5, m, tuple(x / 16.0 for x in m), precision=precision)
     finally:
         if old is None:
-            del os.environ["LFTS_HOST_MIX"]
+            del os.environ["LFTS_DEVICE_MIX"]
         else:
-            os.environ["LFTS_HOST_MIX"] = old
+            os.environ["LFTS_DEVICE_MIX"] = old
     if tiles:
         s.set_tiles(**tiles)
     return s

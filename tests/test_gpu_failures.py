@@ -33,18 +33,18 @@ def lfts(native_lib):
 
 @pytest.fixture(params=["device", "host"])
 def system(lfts, request):
-    """A 16^3 context with its Anderson loop on the device (the default) or
-    on the host (LFTS_HOST_MIX=1)."""
+    """A 16^3 context with its Anderson loop on the device or
+    on the host (the default; LFTS_DEVICE_MIX=1 selects the device loop)."""
     def make(precision):
-        old = os.environ.get("LFTS_HOST_MIX")
-        os.environ["LFTS_HOST_MIX"] = "1" if request.param == "host" else "0"
+        old = os.environ.get("LFTS_DEVICE_MIX")
+        os.environ["LFTS_DEVICE_MIX"] = "1" if request.param == "device" else "0"
         try:
             return lfts.System(N, NA, 12.0, 50.0, 0.5, M3, L, precision=precision)
         finally:
             if old is None:
-                del os.environ["LFTS_HOST_MIX"]
+                del os.environ["LFTS_DEVICE_MIX"]
             else:
-                os.environ["LFTS_HOST_MIX"] = old
+                os.environ["LFTS_DEVICE_MIX"] = old
     return make
 
 
