@@ -584,7 +584,9 @@ def main(argv=None):
     ms_calc = time_calc_concs(fp32_sys, torch, device)
     fp32_sys.close()
     fp64 = run_precision(lfts, lfts.LFTS_FP64, args.steps, args.warmup, rank, device, torch, None)
-    fp64.pop("system").close()
+    fp64_sys = fp64.pop("system")
+    tiles64 = fp64_sys.tiles()
+    fp64_sys.close()
     ms64 = max_over_ranks(torch, fp64["ms_per_step"], device)
     e2e64 = max_over_ranks(torch, fp64["e2e_ms_per_step"], device)
 
@@ -683,7 +685,7 @@ def main(argv=None):
                              "h2d_bytes_per_step": fp64["h2d_bytes_per_step"],
                              "d2h_bytes_per_step": fp64["d2h_bytes_per_step"],
                              "same_anderson_K": fp64["e2e_same_K"]},
-                     "ms_plane": fp64["profile"][0], "ms_pencil": fp64["profile"][1],
+                     "ms_plane": fp64["profile"][0], "ms_pencil": fp64["profile"][1], "tiles": tiles64,
                      "calc_concs_per_s": fp64["calc_concs_per_step"] * 1e3 / ms64},
             "speedup_fp32_mixed_vs_fp64": ms64 / ms32,
             "fp32_err_vs_fp64": errs,
