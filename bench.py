@@ -376,13 +376,22 @@ def ensemble_bench(lfts, torch, device, steps=5, warmup=3):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    e.run(steps, CFG["max_iter"], CFG["tol"], record_k=False)
+    ks, _ = e.run(steps, CFG["max_iter"], CFG["tol"], record_k=True)
     ev1.record(stream)
     ev1.synchronize()
     ms = ev0.elapsed_time(ev1) / steps
     K = ks.astype(float) - 1.0  # mix returns iterations + 1
     N = reps[0]["N"]
     point_steps = sum(float(np.prod(d["m"])) * (N - 1) * (K[:, r].mean() + 1.0) for r, d in enumerate(reps))
+    # algorithmic bytes of the timed steps, replica by replica, with the
+    # single-context formula: (K+1) W_cc + K W_am + 7M, FP32-mixed word sizes
+    alg = 0.0
+    for r, d in enumerate(reps):
+        M = float(np.prod(d["m"]))
+        Kr = float(K[:, r].mean())
+        alg += (Kr + 1.0) * (7 * d["N"] * M * 4 + 6 * M * 8) + Kr * (3 * 10 + 7) * M * 8 + 7 * M * 8
+    peak, peak_kind = measured_peak()
+    achieved = alg / (ms * 1e-3) / 1e9
     seq_ms = sequential_single_contexts(lfts, torch, device, reps, fields)
     out = {"replicas": len(reps), "meshes": {str(mm): int(sum(1 for d in reps if d["m"][0] == mm))
                                              for mm in (32, 48, 64, 96)},
@@ -390,6 +399,10 @@ def ensemble_bench(lfts, torch, device, steps=5, warmup=3):
            "mean_anderson_K": float(K.mean()),
            "mesh_point_contour_steps_per_s": point_steps * 1e3 / ms,
            "tiles": {str(d["m"][0]): e.tiles(r) for r, d in enumerate(reps)},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "peak_kind": peak_kind, "algorithmic_bytes_per_step": alg,
+                        "unit_of_work": "one Langevin step of every replica, sum over replicas of (K+1) W_cc + "
+                                        "K W_am + 7M with each replica's own M, N and K"},
            "timing": f"{steps} steps after {warmup} warm-up steps, the timed steps as one CUDA graph launch",
            "sequential_single_contexts_ms_per_step": seq_ms,
            "speedup_vs_sequential_single_contexts": seq_ms / ms}

@@ -35,6 +35,9 @@ namespace lfts {
 // own CTAs are running.  Launched without the attribute, both are no-ops.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+// pull one 128-byte line into L2 (a hint: L2 is the point of coherence, so a
+// line fetched before its last writer finished is still read current)
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
 enum PlaneMode : int {
     PLANE_INIT_W = 0,  // h = exp(-w/N) from the fields, store h, forward transform
@@ -61,6 +64,7 @@ struct PlaneArgs {
     int nchains;
     double Nd;            // N as a double (h = exp(-w/N))
     const T *gx, *gy, *gz;  // PLANE_G: separable Boltzmann weight, 1/M folded into gz
+    const T *pf;          // PLANE_G: (chain 1, chain 2) slot that the next x-pencil reads, pulled into L2
 };
 
 template <typename T, int NY, int NZ>

@@ -292,6 +292,14 @@ __device__ __forceinline__ void plane3_body(const PlaneArgs<float> &a, const int
     } else if (MODE == PLANE_G && threadIdx.x < C::NY + 2 * C::NZ) {
         GZ[threadIdx.x - C::NY - C::NZ] = a.gz[threadIdx.x - C::NY - C::NZ];
     }
+    // The summing x-pencil after this launch reads a stored slot written many
+    // steps earlier, long gone from L2; this plane's share of it (plane x, one
+    // float pair per point) is fetched into L2 while the transforms run.
+    if (MODE == PLANE_G && a.pf) {
+        const char *base = reinterpret_cast<const char *>(a.pf + 2 * plane_off);
+        constexpr int BYTES = 2 * C::NY * C::NZ * (int)sizeof(float);
+        for (int o = 128 * threadIdx.x; o < BYTES; o += 128 * C::NT) prefetch_l2(base + o);
+    }
     pdl_launch_dependents();
     pdl_wait();
 

@@ -321,7 +321,9 @@ void enqueue_chain_launches(lfts_ctx *c)
             const bool acc = c->phi_in_chain;
             bool first_acc = true;
             for (int i = 1; i < c->N; i++) {
-                launch_plane<T>(c, PLANE_G, a, 2);
+                PlaneArgs<T> ag = a;
+                if (acc && c->N - i < i + 1) ag.pf = q + (long long)(c->N - i - 1) * 2 * M;  // the partner slot
+                launch_plane<T>(c, PLANE_G, ag, 2);
                 PencilArgs<T> ph = pa;
                 ph.qout = q + (long long)i * 2 * M;  // slot i+1
                 ph.hsel0 = hsel_chain0(c, i);
