@@ -654,7 +654,7 @@ def main(argv=None):
             traffic = tj.get("bytes_per_step_fp32_128")
             traffic_cc = tj.get("bytes_per_calc_concs_fp32_128", {}).get("phi_in_chain" if tiles32.get(
                 "phi_in_chain") else "separate_pass")
-        # the roofline unit SURVEY-style: one calc_concs (the contour chain, Q
+        # the roofline unit: one calc_concs (the contour chain, Q
         # and the concentrations), algorithmic bytes W_cc = 7 N M propagator
         # words (FP32) + 6 M field words (FP64): read q, read h, write q per
         # chain step, the N stored propagators read back for phi, w in, h and

@@ -1,4 +1,4 @@
-"""TEST AND BASELINE INFRASTRUCTURE ONLY -- the reference's calc_concs
+"""TEST AND CPU-TIMING INFRASTRUCTURE ONLY -- the reference's calc_concs
 (src/diblock.cc:30-60 with step::fwd, src/step.cc:35-65, and normalize_phi,
 src/diblock.cc:85-95) restated on scipy.fft (pocketfft) with `workers`
 threads and in-place numpy arithmetic.
