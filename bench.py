@@ -595,6 +595,13 @@ def main(argv=None):
     part_chain, part_conc, part_upd = fp32_sys.profile_iteration(5)
     tiles32 = fp32_sys.tiles()
     ms_calc = time_calc_concs(fp32_sys, torch, device)
+    # the contour step of a chain that stores every slot (the tuned chain may
+    # form the concentration sums in its second half instead)
+    ch_storing = None
+    if tiles32.get("phi_in_chain"):
+        fp32_sys.set_tiles(**dict(tiles32, phi_in_chain=0))
+        ch_storing = min(fp32_sys.profile_chain()[2] for _ in range(3))
+        fp32_sys.set_tiles(**tiles32)
     fp32_sys.close()
     fp64 = run_precision(lfts, lfts.LFTS_FP64, args.steps, args.warmup, rank, device, torch, None)
     fp64_sys = fp64.pop("system")
@@ -682,8 +689,13 @@ def main(argv=None):
                                       "peak_kind": peak_kind, "traffic": traffic,
                                       "algorithmic_bytes_per_launch": step_bytes, "ms_per_step": step_ms,
                                       "ms_plane_alone": pl, "ms_pencil_alone": pe,
+                                      "storing_chain": None if ch_storing is None else {
+                                          "ms_per_step": ch_storing / (N - 1),
+                                          "achieved": step_bytes / (ch_storing / (N - 1) * 1e-3) / 1e9,
+                                          "frac": step_bytes / (ch_storing / (N - 1) * 1e-3) / 1e9 / peak},
                                       "note": "with phi_in_chain the second half of the steps also reads the "
-                                              "partner slots and adds the concentration sums (not in these bytes)"},
+                                              "partner slots and adds the concentration sums (not in these bytes); "
+                                              "storing_chain: the same step in a chain that stores every slot"},
             "cpu_baseline": cpu,
             "clocks": fp32["clocks"],
             "gpu_launches": fp32["launches"],
