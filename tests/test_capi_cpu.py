@@ -93,3 +93,27 @@ def test_read_input_rejects_zero_sample_freq(native_lib, tmp_path):
     write_input(p, ["64 32 14.0 50.0 0.5 0", "32 32 32 4.0 4.0 4.0", "10 10 0 1000 0"])
     with pytest.raises(LftsError):
         read_input(p)
+
+
+@pytest.mark.parametrize("kw,status", [
+    (dict(N=1, NA=1), 1),                    # a chain needs two monomers
+    (dict(NA=9), 1),                         # NA > N
+    (dict(NA=-1), 1),
+    (dict(C_=0.0), 1),
+    (dict(XbN=0.0), 1),
+    (dict(L=(3.0, 0.0, 3.0)), 1),            # box length not positive
+    (dict(L=(3.0, float("nan"), 3.0)), 1),
+    (dict(precision=7), 1),                  # neither FP64 nor FP32-mixed
+    (dict(m=(17, 16, 16)), 2),               # no FFT plan for 17
+    (dict(m=(16, 15, 16)), 2),               # odd my
+])
+def test_create_rejects_bad_parameters_before_any_device_call(native_lib, kw, status):
+    """lfts_create validates its parameters first: bad ones give
+    LFTS_ERR_ARG (1) or LFTS_ERR_UNSUPPORTED (2) on any machine, while valid
+    ones get as far as the device query (LFTS_ERR_CUDA without a GPU)."""
+    from lfts_cpu_b200 import LftsError, System
+    args = dict(N=8, NA=4, XbN=10.0, C_=50.0, dt=0.5, m=(16, 16, 16), L=(3.0, 3.0, 3.0), precision=0)
+    args.update(kw)
+    with pytest.raises(LftsError) as e:
+        System(**args)
+    assert e.value.status == status
