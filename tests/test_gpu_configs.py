@@ -1,13 +1,16 @@
 """Parity at the benchmark configurations' own sizes (N = 64), against
 fixtures made by the reference itself (tests/golden/make_golden.py, cases
-cfg1_32, cfg2_64, cfg4_64; 4M field arrays kept as every stride-th value plus
-per-quarter sums):
+cfg1_32, cfg2_64, cfg3_128, cfg4_64; 4M field arrays kept as every stride-th
+value plus per-quarter sums):
 
 * the plain-FP64 CPU configuration: 32^3, N=64, NA=32, XN=14, C=50, dt=0.5,
   L=4, seeded Gaussian (sd 0.01) start fed as loadType 1; initial mix and 10
   Langevin steps with S(k) sampled every step;
 * the plain-FP64 B200 configuration: 64^3, N=64, NA=32, XN=16, C=100,
   L=6.4, (300) lamellar start; initial mix and 3 steps;
+* the mixed-precision B200 configuration at its own size: 128^3, N=64, NA=25,
+  XN=20, C=100, dt=0.5, L=8, the bench's seeded Gaussian (sd 0.01) start;
+  initial mix and one Langevin step with S(k) sampled;
 * the adjoint configuration: 64^3, N=64, NA=32, XN=15, C=50, L=6.0,
   lamellar; one step, then H, phi and the backward pass.
 
@@ -87,7 +90,7 @@ def sensitive(g):
             or list(g["K_perturbed"]) != list(g["K"]))
 
 
-@pytest.mark.parametrize("name", ["cfg1_32", "cfg2_64", "cfg4_64"])
+@pytest.mark.parametrize("name", ["cfg1_32", "cfg2_64", "cfg3_128", "cfg4_64"])
 @pytest.mark.parametrize("precision", [0, 1])
 def test_config_calc_concs_of_the_start(lfts, name, precision):
     g, hdr, M, s = setup(lfts, name, precision)
@@ -118,7 +121,7 @@ def run_trajectory(lfts, g, hdr, M, s):
     return w0, Ks, np.array(lnQs)
 
 
-@pytest.mark.parametrize("name", ["cfg1_32", "cfg2_64", "cfg4_64"])
+@pytest.mark.parametrize("name", ["cfg1_32", "cfg2_64", "cfg3_128", "cfg4_64"])
 def test_config_trajectory_fp64(lfts, name):
     """Initial mix and Langevin steps with the reference's noise stream: the
     mixed start, K per step, ln Q per step, fields, S(k) and its binned text,
