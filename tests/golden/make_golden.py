@@ -256,6 +256,31 @@ def case_program_run(name, hdr):
         shutil.rmtree(work, ignore_errors=True)
 
 
+def case_program_compact(name, src_input, every=997):
+    """The reference program (oracle/_ref/lfts-ref) on one of the reference's own
+    input files, for meshes whose output files are too large to keep: its
+    stdout, and per output file the line count and every `every`-th line
+    (lines 0, every, 2 every, ...), in tests/golden/<name>.npz."""
+    import subprocess
+    from pyoracle import REF_BIN
+    work = tempfile.mkdtemp()
+    try:
+        shutil.copy(src_input, os.path.join(work, "input"))
+        out = subprocess.run([REF_BIN, "input"], cwd=work, capture_output=True, text=True,
+                             env=dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count())), check=True).stdout
+        files = sorted(f for f in os.listdir(work) if f != "input")
+        rec = {"input": open(os.path.join(work, "input")).read(), "stdout": out, "files": np.array(files),
+               "every": every}
+        for f in files:
+            lines = open(os.path.join(work, f)).read().splitlines()
+            rec["n_" + f] = len(lines)
+            rec["s_" + f] = np.array(lines[::every])
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **rec)
+        print(name, files, [rec["n_" + f] for f in files])
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
 CASES = {
     "comp_16": lambda: case_components("comp_16", 6, 10, (16, 16, 16), (3.2, 3.0, 3.4), 11, 2.0, 0.5),
     "comp_12x24x16": lambda: case_components("comp_12x24x16", 7, 9, (12, 24, 16), (2.5, 4.1, 3.3), 12, 1.5, 0.3,
@@ -281,6 +306,11 @@ CASES = {
     # a disordered-start run that saves and samples every step
     "prog_saves16": lambda: case_program_run(
         "prog_saves16", ((16, 6, 12.0, 50.0, 0.5, 0), ((16, 16, 16), (3.0, 3.0, 3.0)), (2, 2, 1, 1, 0))),
+    # the reference's own 128^3 input (input_files/input128: N=90, NA=40,
+    # XeN=13.15 with isXeN=1, random start, 2 equilibration steps), run by the
+    # reference program; its 2M-line field files kept as every 997th line
+    "prog_input128": lambda: case_program_compact(
+        "prog_input128", os.path.join(REF_TREE, "input_files", "input128")),
     # plain-FP64 configuration, CPU-runnable: 32^3, N=64, NA=32, XN=14, C=50,
     # dt=0.5, L=4, seeded Gaussian (sd 0.01) start; initial mix + 10 steps,
     # S(k) sampled every step

@@ -30,9 +30,11 @@ def _values(lines):
 MAX_FLIPS = 2  # lines per file whose 6th significant digit may round the other way
 
 
-def compare_text(got, ref, name):
+def compare_text(got, ref, name, max_flips=MAX_FLIPS, floor_frac=0.0):
     """Line for line; returns the number of lines whose text differs (each a
-    last-digit rounding flip of a value within 2e-5 of the reference's)."""
+    last-digit rounding flip of a value within 2e-5 of the reference's,
+    relative to the larger of its magnitude, 1e-3 and floor_frac times the
+    largest magnitude in the file)."""
     g = got.splitlines()
     r = ref.splitlines()
     assert len(g) == len(r), f"{name}: {len(g)} lines vs {len(r)}"
@@ -41,9 +43,10 @@ def compare_text(got, ref, name):
     assert gv.shape == rv.shape, name
     finite = np.isfinite(rv)
     assert np.array_equal(np.isfinite(gv), finite), name
-    rel = np.abs(gv[finite] - rv[finite]) / np.maximum(np.abs(rv[finite]), 1e-3)
+    floor = max(1e-3, floor_frac * float(np.max(np.abs(rv[finite]), initial=0.0)))
+    rel = np.abs(gv[finite] - rv[finite]) / np.maximum(np.abs(rv[finite]), floor)
     assert rel.max() < 2e-5, f"{name}: max rel diff {rel.max()}"
-    assert flips <= MAX_FLIPS, f"{name}: {flips} of {len(r)} lines differ in text"
+    assert max_flips is None or flips <= max_flips, f"{name}: {flips} of {len(r)} lines differ in text"
     return flips
 
 
@@ -75,3 +78,37 @@ def test_driver_reproduces_reference_outputs(native_lib, tmp_path, name):
     # banner that only an OpenMP build of the reference prints
     keep = lambda s: [ln for ln in s.splitlines() if "time =" not in ln and "threads for FFTs" not in ln]
     compare_text("\n".join(keep(r.stdout)), "\n".join(keep((ref / "stdout.txt").read_text())), "stdout")
+
+
+@pytest.mark.gpu
+def test_driver_on_the_reference_128_input(native_lib, tmp_path):
+    """The reference's own input_files/input128 (128^3, N=90, NA=40, XeN=13.15
+    with isXeN=1, random start, 2 equilibration steps) against the reference
+    program's run of it (tests/golden/prog_input128.npz): stdout line for line,
+    and per output file the line count and every 997th line (the field files
+    have 2M lines each).  The Anderson counts and ln Q in stdout must match as
+    in the tests above.  The field values must be within 2e-7 of the file's
+    largest magnitude of the reference's; their 6-digit text is counted, not
+    required equal: the reference's own Anderson mix is reproducible only to
+    about 1e-8 at this size (its mixed w+ moves by 3.6e-8 under a 1e-15
+    perturbation of the start, tests/golden/cfg3_128.npz), and the small w+
+    values print that difference in their 6th digit."""
+    g = np.load(os.path.join(GOLDEN, "prog_input128.npz"))
+    (tmp_path / "input").write_text(str(g["input"]))
+    r = subprocess.run([EXE, "input"], cwd=tmp_path, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr
+    files = [str(f) for f in g["files"]]
+    produced = sorted(f for f in os.listdir(tmp_path) if f != "input")
+    assert produced == files
+    every = int(g["every"])
+    flips = {}
+    for f in files:
+        lines = (tmp_path / f).read_text().splitlines()
+        assert len(lines) == int(g["n_" + f]), f
+        sampled = [str(x) for x in g["s_" + f]]
+        flips[f] = compare_text("\n".join(lines[::every]), "\n".join(sampled), f,
+                                max_flips=None, floor_frac=1e-2)
+    print(f"prog_input128: sampled text lines differing per file {flips} "
+          f"of {len(g['s_' + files[0]])} each")
+    keep = lambda s: [ln for ln in s.splitlines() if "time =" not in ln and "threads for FFTs" not in ln]
+    compare_text("\n".join(keep(r.stdout)), "\n".join(keep(str(g["stdout"]))), "stdout")
