@@ -311,6 +311,9 @@ CASES = {
     # reference program; its 2M-line field files kept as every 997th line
     "prog_input128": lambda: case_program_compact(
         "prog_input128", os.path.join(REF_TREE, "input_files", "input128")),
+    # the same at 64^3 (input_files/input64)
+    "prog_input64": lambda: case_program_compact(
+        "prog_input64", os.path.join(REF_TREE, "input_files", "input64"), every=97),
     # plain-FP64 configuration, CPU-runnable: 32^3, N=64, NA=32, XN=14, C=50,
     # dt=0.5, L=4, seeded Gaussian (sd 0.01) start; initial mix + 10 steps,
     # S(k) sampled every step

@@ -81,19 +81,20 @@ def test_driver_reproduces_reference_outputs(native_lib, tmp_path, name):
 
 
 @pytest.mark.gpu
-def test_driver_on_the_reference_128_input(native_lib, tmp_path):
-    """The reference's own input_files/input128 (128^3, N=90, NA=40, XeN=13.15
-    with isXeN=1, random start, 2 equilibration steps) against the reference
-    program's run of it (tests/golden/prog_input128.npz): stdout line for line,
-    and per output file the line count and every 997th line (the field files
-    have 2M lines each).  The Anderson counts and ln Q in stdout must match as
+@pytest.mark.parametrize("name", ["prog_input64", "prog_input128"])
+def test_driver_on_the_reference_inputs(native_lib, tmp_path, name):
+    """The reference's own input_files/input64 and input128 (64^3 and 128^3,
+    N=90, NA=40, XeN=13.15 with isXeN=1, random start, 2 equilibration steps)
+    against the reference program's runs of them (tests/golden/<name>.npz):
+    stdout line for line, and per output file the line count and every 97th
+    (64^3) or 997th (128^3) line (the field files have 2M lines at 128^3).  The Anderson counts and ln Q in stdout must match as
     in the tests above.  The field values must be within 2e-7 of the file's
     largest magnitude of the reference's; their 6-digit text is counted, not
     required equal: the reference's own Anderson mix is reproducible only to
     about 1e-8 at this size (its mixed w+ moves by 3.6e-8 under a 1e-15
     perturbation of the start, tests/golden/cfg3_128.npz), and the small w+
     values print that difference in their 6th digit."""
-    g = np.load(os.path.join(GOLDEN, "prog_input128.npz"))
+    g = np.load(os.path.join(GOLDEN, name + ".npz"))
     (tmp_path / "input").write_text(str(g["input"]))
     r = subprocess.run([EXE, "input"], cwd=tmp_path, capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stderr
@@ -108,7 +109,7 @@ def test_driver_on_the_reference_128_input(native_lib, tmp_path):
         sampled = [str(x) for x in g["s_" + f]]
         flips[f] = compare_text("\n".join(lines[::every]), "\n".join(sampled), f,
                                 max_flips=None, floor_frac=1e-2)
-    print(f"prog_input128: sampled text lines differing per file {flips} "
+    print(f"{name}: sampled text lines differing per file {flips} "
           f"of {len(g['s_' + files[0]])} each")
     keep = lambda s: [ln for ln in s.splitlines() if "time =" not in ln and "threads for FFTs" not in ln]
     compare_text("\n".join(keep(r.stdout)), "\n".join(keep(str(g["stdout"]))), "stdout")
