@@ -223,6 +223,7 @@ class RefHarness:
             lib.ref_lgv_create.restype = C.c_void_p
             lib.ref_lgv_create.argtypes = [C.c_ulonglong, C.c_double, C.c_int]
             lib.ref_lgv_destroy.argtypes = [C.c_void_p]
+            lib.ref_lgv_uniform_field.argtypes = [C.c_void_p, C.c_double, C.c_int, _dp]
             lib.ref_sys_full_step.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double, _dp,
                                               C.POINTER(C.c_int), C.POINTER(C.c_double)]
             cls._lib = lib
@@ -287,6 +288,13 @@ class RefLangevin:
             self._l = None
 
     __del__ = close
+
+    def uniform_field(self, XbN, M):
+        """W-, w+ (2M) of the reference program's random start (loadType 0 or
+        3), drawn from this generator after the constructor's noise"""
+        w = np.zeros(2 * int(M))
+        self._lib.ref_lgv_uniform_field(self._l, float(XbN), int(M), w)
+        return w
 
     def full_step(self, sys_: RefSys, w, XbN, dt):
         K = C.c_int()

@@ -103,6 +103,19 @@ ref_lgv *ref_lgv_create(unsigned long long seed, double sigma, int M)
 
 void ref_lgv_destroy(ref_lgv *l) { delete l; }
 
+/* lfts_simulation::generate_field's default branch (src/lfts_simulation.cc:
+ * 150-154), drawing from this object's generator after the langevin
+ * constructor's draws, as the reference's program does: W- = XbN (U - 0.5),
+ * w+ = 0, into w[0, 2M) */
+void ref_lgv_uniform_field(ref_lgv *l, double XbN, int M, double *w)
+{
+    std::uniform_real_distribution<double> u(0.0, 1.0);
+    for (int r = 0; r < M; r++) {
+        w[r] = XbN * (u(l->rng) - 0.5);
+        w[r + M] = 0.0;
+    }
+}
+
 void ref_sys_full_step(ref_sys *s, ref_lgv *l, double XbN, double sigma, double dt, double *w, int *K,
                        double *lnQ)
 {

@@ -281,6 +281,56 @@ def case_program_compact(name, src_input, every=997):
         shutil.rmtree(work, ignore_errors=True)
 
 
+def case_program_spread(name, src_input, every=997):
+    """How reproducible the reference program's w_0 / phi_0 (the fields after
+    its initial Anderson mix, src/lfts_simulation.cc:52-56) are on one of its
+    own inputs: its random start (the program's generator, after the langevin
+    constructor's draws) mixed twice by the reference's objects, as is and
+    times (1 + 1e-15); the 6-significant-digit text of the two results is
+    compared value by value, over all values and over the lines the compact
+    program fixture keeps (every `every`-th line of the file).  The first run
+    must equal the program's own w_0 bit for bit."""
+    from pyoracle import RefLangevin
+    work = tempfile.mkdtemp()
+    cwd = os.getcwd()
+    try:
+        os.chdir(work)
+        shutil.copy(src_input, "input")
+        RefHarness.lib().ref_set_threads(os.cpu_count())
+        sim = RefSim("input")
+        w_prog = sim.w()
+        M, N, NA, XbN, sigma = sim.M, sim.N, sim.NA, sim.XbN, sim.sigma
+        m = list(sim.m)
+        L = [float(x) for x in open("input").read().split("\n")[1].split()[3:6]]
+        sim.close()
+    finally:
+        os.chdir(cwd)
+        shutil.rmtree(work, ignore_errors=True)
+    lg = RefLangevin(123456789, sigma, M)
+    start = lg.uniform_field(XbN, M)
+    lg.close()
+    runs = []
+    for eps in (0.0, 1e-15):
+        s2 = RefSys(NA, N - NA, m, L)
+        w = np.zeros(4 * M)
+        w[:2 * M] = start * (1.0 + eps)
+        s2.mix(w)
+        runs.append(w)
+        s2.close()
+    assert np.array_equal(runs[0], w_prog), "the harness start is not the program's"
+    text = lambda a: np.array(["%g" % v for v in a])  # noqa: E731  (the files' default 6 digits)
+    out = {"every": every, "spread": np.abs(runs[0] - runs[1]).reshape(4, M).max(axis=1)}
+    for f, lo, hi, header in (("w_0", 0, 2 * M, 3), ("phi_0", 2 * M, 4 * M, 0)):
+        ta, tb = text(runs[0][lo:hi]), text(runs[1][lo:hi])
+        diff = ta != tb
+        lines = np.arange(header, header + (hi - lo))  # file line of each value
+        out["flips_all_" + f] = int(diff.sum())
+        out["flips_sampled_" + f] = int(diff[lines % every == 0].sum())
+        out["n_sampled_" + f] = int((lines % every == 0).sum())
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, {k: v for k, v in out.items()})
+
+
 CASES = {
     "comp_16": lambda: case_components("comp_16", 6, 10, (16, 16, 16), (3.2, 3.0, 3.4), 11, 2.0, 0.5),
     "comp_12x24x16": lambda: case_components("comp_12x24x16", 7, 9, (12, 24, 16), (2.5, 4.1, 3.3), 12, 1.5, 0.3,
@@ -311,6 +361,11 @@ CASES = {
     # reference program; its 2M-line field files kept as every 997th line
     "prog_input128": lambda: case_program_compact(
         "prog_input128", os.path.join(REF_TREE, "input_files", "input128")),
+    # the reference's own reproducibility of that run's w_0 / phi_0
+    "spread_input128": lambda: case_program_spread(
+        "spread_input128", os.path.join(REF_TREE, "input_files", "input128")),
+    "spread_input64": lambda: case_program_spread(
+        "spread_input64", os.path.join(REF_TREE, "input_files", "input64"), every=97),
     # the same at 64^3 (input_files/input64)
     "prog_input64": lambda: case_program_compact(
         "prog_input64", os.path.join(REF_TREE, "input_files", "input64"), every=97),

@@ -87,14 +87,20 @@ def test_driver_on_the_reference_inputs(native_lib, tmp_path, name):
     N=90, NA=40, XeN=13.15 with isXeN=1, random start, 2 equilibration steps)
     against the reference program's runs of them (tests/golden/<name>.npz):
     stdout line for line, and per output file the line count and every 97th
-    (64^3) or 997th (128^3) line (the field files have 2M lines at 128^3).  The Anderson counts and ln Q in stdout must match as
-    in the tests above.  The field values must be within 2e-7 of the file's
-    largest magnitude of the reference's; their 6-digit text is counted, not
-    required equal: the reference's own Anderson mix is reproducible only to
-    about 1e-8 at this size (its mixed w+ moves by 3.6e-8 under a 1e-15
-    perturbation of the start, tests/golden/cfg3_128.npz), and the small w+
-    values print that difference in their 6th digit."""
+    (64^3) or 997th (128^3) line (the field files have 2M lines at 128^3).
+    The Anderson counts and ln Q in stdout must match as in the tests above,
+    and every sampled field value be within 2e-7 of the file's largest
+    magnitude.  Their 6-digit text cannot all match, because the reference's
+    own run is not that reproducible: tests/golden/spread_<input>.npz records
+    the reference mixing its start twice, as is and perturbed by 1e-15, and at
+    128^3 its w+ moves by 1.2e-7 and 185 of the 4206 sampled lines of its own
+    w_0 print differently.  So w_0 and phi_0 may differ in at most 5 times
+    the reference's own count of sampled lines (plus MAX_FLIPS), the later
+    files in at most MAX_FLIPS plus one per thousand sampled lines; the
+    counts are printed."""
     g = np.load(os.path.join(GOLDEN, name + ".npz"))
+    sp = np.load(os.path.join(GOLDEN, name.replace("prog_", "spread_") + ".npz"))
+    assert int(sp["every"]) == int(g["every"])
     (tmp_path / "input").write_text(str(g["input"]))
     r = subprocess.run([EXE, "input"], cwd=tmp_path, capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stderr
@@ -107,9 +113,13 @@ def test_driver_on_the_reference_inputs(native_lib, tmp_path, name):
         lines = (tmp_path / f).read_text().splitlines()
         assert len(lines) == int(g["n_" + f]), f
         sampled = [str(x) for x in g["s_" + f]]
-        flips[f] = compare_text("\n".join(lines[::every]), "\n".join(sampled), f,
-                                max_flips=None, floor_frac=1e-2)
-    print(f"{name}: sampled text lines differing per file {flips} "
-          f"of {len(g['s_' + files[0]])} each")
+        if "flips_sampled_" + f in sp:
+            cap = 5 * int(sp["flips_sampled_" + f]) + MAX_FLIPS
+        else:
+            cap = MAX_FLIPS + len(sampled) // 1000
+        flips[f] = compare_text("\n".join(lines[::every]), "\n".join(sampled), f, max_flips=cap, floor_frac=1e-2)
+    print(f"{name}: sampled text lines differing per file {flips} of {len(g['s_' + files[0]])} each; "
+          f"the reference against itself: w_0 {int(sp['flips_sampled_w_0'])}, "
+          f"phi_0 {int(sp['flips_sampled_phi_0'])}")
     keep = lambda s: [ln for ln in s.splitlines() if "time =" not in ln and "threads for FFTs" not in ln]
     compare_text("\n".join(keep(r.stdout)), "\n".join(keep(str(g["stdout"]))), "stdout")
