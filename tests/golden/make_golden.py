@@ -281,6 +281,60 @@ def case_program_compact(name, src_input, every=997):
         shutil.rmtree(work, ignore_errors=True)
 
 
+def case_long_run(name, hdr, field_seed, blocks=10):
+    """A whole run of the reference at one configuration (its n_eq
+    equilibration and n_st statistics steps, S(k) sampled every n_smpl
+    statistics steps), kept as what a long run is compared by: K, ln Q and
+    H = -ln Q + (sum W-^2 / XbN - sum w+)/M per step, and the binned S(k) of
+    each of `blocks` equal blocks of the statistics steps (binned with the
+    oracle's restatement of strFunc::save, checked here against the
+    reference's own struct file for the whole accumulation)."""
+    from pyoracle import Oracle
+    (N, NA, XN, C, dt, isXeN), (m, L), (neq, nst, nsm, sf, lt) = hdr
+    M = int(np.prod(m))
+    fields = np.random.default_rng(field_seed).normal(0.0, 0.01, 2 * M)
+    work = tempfile.mkdtemp()
+    cwd = os.getcwd()
+    try:
+        os.chdir(work)
+        write_input("input", hdr, fields)
+        RefHarness.lib().ref_set_threads(os.cpu_count())
+        sim = RefSim("input")
+        XbN, CV = sim.XbN, sim.CV
+        Ks, lnQs, Hs = [], [], []
+        S_prev, ns_prev = np.zeros(sim.Mk), 0
+        per_block = nst // blocks
+        Sb_blocks, K_bins = [], None
+        for it in range(1, neq + nst + 1):
+            st = it > neq
+            k, lq = sim.step(sample=st and ((it - neq) % nsm == 0))
+            w = sim.w()
+            Ks.append(k)
+            lnQs.append(lq)
+            Hs.append(-lq + (np.sum(w[:M] ** 2) / XbN - np.sum(w[M:2 * M])) / M)
+            if st and (it - neq) % per_block == 0:
+                S, ns = sim.sk_raw()
+                Kb, Sb = Oracle.sk_bin(m, L, S - S_prev, ns - ns_prev, CV, XbN)
+                K_bins = Kb
+                Sb_blocks.append(Sb)
+                S_prev, ns_prev = S.copy(), ns
+        S, ns = sim.sk_raw()
+        sim.sk_save("struct_out")
+        ref = np.array([[float(v) for v in ln.split("\t")] for ln in open("struct_out").read().strip().split("\n")])
+        Kb, Sb = Oracle.sk_bin(m, L, S, ns, CV, XbN)
+        assert len(Kb) == len(ref) and np.max(np.abs(Kb - ref[:, 0])) < 1e-8
+        assert np.max(np.abs(Sb - ref[:, 1])) < 1e-7 * max(1.0, np.max(np.abs(ref[:, 1])))
+        sim.close()
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), K=np.array(Ks), lnQ=np.array(lnQs), H=np.array(Hs),
+                            K_bins=K_bins, Sb_blocks=np.array(Sb_blocks), field_seed=field_seed, n_eq=neq,
+                            n_st=nst, n_smpl=nsm, blocks=blocks, XbN=XbN, CV=CV, sigma=sim.sigma, N=N, NA=NA,
+                            m=np.array(m), L=np.array(L), C=C, dt=dt)
+        print(name, "mean K", np.mean(Ks), "H st mean", np.mean(Hs[neq:]), "bins", len(K_bins))
+    finally:
+        os.chdir(cwd)
+        shutil.rmtree(work, ignore_errors=True)
+
+
 def case_program_spread(name, src_input, every=997):
     """How reproducible the reference program's w_0 / phi_0 (the fields after
     its initial Anderson mix, src/lfts_simulation.cc:52-56) are on one of its
@@ -369,6 +423,11 @@ CASES = {
     # the same at 64^3 (input_files/input64)
     "prog_input64": lambda: case_program_compact(
         "prog_input64", os.path.join(REF_TREE, "input_files", "input64"), every=97),
+    # the plain-FP64 CPU configuration run whole (1000 + 1000 steps, S(k)
+    # every 10th statistics step) for the long-run statistics
+    "long_cfg1": lambda: case_long_run(
+        "long_cfg1", ((64, 32, 14.0, 50.0, 0.5, 0), ((32, 32, 32), (4.0, 4.0, 4.0)), (1000, 1000, 10, 1000000, 1)),
+        101),
     # plain-FP64 configuration, CPU-runnable: 32^3, N=64, NA=32, XN=14, C=50,
     # dt=0.5, L=4, seeded Gaussian (sd 0.01) start; initial mix + 10 steps,
     # S(k) sampled every step
