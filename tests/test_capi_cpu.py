@@ -117,3 +117,24 @@ def test_create_rejects_bad_parameters_before_any_device_call(native_lib, kw, st
     with pytest.raises(LftsError) as e:
         System(**args)
     assert e.value.status == status
+
+
+def _replica(**kw):
+    d = dict(N=16, NA=8, XbN=12.0, C=50.0, dt=0.5, m=(32, 32, 32), L=(2.0, 2.0, 2.0), seed=1)
+    d.update(kw)
+    return d
+
+
+@pytest.mark.parametrize("reps,status", [
+    ([], 1),                                               # no replicas
+    ([_replica(), _replica(N=12, NA=6)], 1),               # the chain length is shared
+    ([_replica(), _replica(m=(128, 128, 128))], 2),        # ensemble meshes 16..96 per side
+    ([_replica(m=(32, 32, 48))], 2),                       # square yz planes only
+])
+def test_ensemble_create_rejects_bad_replicas_before_any_device_call(native_lib, reps, status):
+    """lfts_ensemble_create checks the replica list first (LFTS_ERR_ARG,
+    LFTS_ERR_UNSUPPORTED) on any machine, before it touches a device."""
+    from lfts_cpu_b200 import Ensemble, LftsError
+    with pytest.raises(LftsError) as e:
+        Ensemble(reps)
+    assert e.value.status == status
