@@ -606,6 +606,7 @@ def main(argv=None):
     fp64 = run_precision(lfts, lfts.LFTS_FP64, args.steps, args.warmup, rank, device, torch, None)
     fp64_sys = fp64.pop("system")
     tiles64 = fp64_sys.tiles()
+    ms_calc64 = time_calc_concs(fp64_sys, torch, device)
     fp64_sys.close()
     ms64 = max_over_ranks(torch, fp64["ms_per_step"], device)
     e2e64 = max_over_ranks(torch, fp64["e2e_ms_per_step"], device)
@@ -711,6 +712,12 @@ def main(argv=None):
                              "d2h_bytes_per_step": fp64["d2h_bytes_per_step"],
                              "same_anderson_K": fp64["e2e_same_K"]},
                      "ms_plane": fp64["profile"][0], "ms_pencil": fp64["profile"][1], "tiles": tiles64,
+                     "roofline": {"bound": "hbm", "kernel": "calc_concs, FP64", "unit": "GB/s", "peak": peak,
+                                  "peak_kind": peak_kind, "ms_per_launch": ms_calc64,
+                                  "algorithmic_bytes_per_launch": 7 * N * M * 8 + 6 * M * 8,
+                                  "achieved": (7 * N * M * 8 + 6 * M * 8) / (ms_calc64 * 1e-3) / 1e9,
+                                  "frac": (7 * N * M * 8 + 6 * M * 8) / (ms_calc64 * 1e-3) / 1e9 / peak,
+                                  "unit_of_work": "one calc_concs, W_cc = 7 N M + 6 M words, all FP64"},
                      "calc_concs_per_s": fp64["calc_concs_per_step"] * 1e3 / ms64},
             "speedup_fp32_mixed_vs_fp64": ms64 / ms32,
             "fp32_err_vs_fp64": errs,
