@@ -656,12 +656,14 @@ def main(argv=None):
                 ens = {"failed": str(e)}
         traffic = None
         traffic_cc = None
+        traffic64 = None
         tp = os.path.join(ROOT, "profiles", "contour_step_traffic.json")
         if os.path.exists(tp):
             tj = json.load(open(tp))
             traffic = tj.get("bytes_per_step_fp32_128")
             traffic_cc = tj.get("bytes_per_calc_concs_fp32_128", {}).get("phi_in_chain" if tiles32.get(
                 "phi_in_chain") else "separate_pass")
+            traffic64 = tj.get("bytes_per_calc_concs_fp64_128")
         # the roofline unit: one calc_concs (the contour chain, Q
         # and the concentrations), algorithmic bytes W_cc = 7 N M propagator
         # words (FP32) + 6 M field words (FP64): read q, read h, write q per
@@ -713,7 +715,7 @@ def main(argv=None):
                              "same_anderson_K": fp64["e2e_same_K"]},
                      "ms_plane": fp64["profile"][0], "ms_pencil": fp64["profile"][1], "tiles": tiles64,
                      "roofline": {"bound": "hbm", "kernel": "calc_concs, FP64", "unit": "GB/s", "peak": peak,
-                                  "peak_kind": peak_kind, "ms_per_launch": ms_calc64,
+                                  "peak_kind": peak_kind, "ms_per_launch": ms_calc64, "traffic": traffic64,
                                   "algorithmic_bytes_per_launch": 7 * N * M * 8 + 6 * M * 8,
                                   "achieved": (7 * N * M * 8 + 6 * M * 8) / (ms_calc64 * 1e-3) / 1e9,
                                   "frac": (7 * N * M * 8 + 6 * M * 8) / (ms_calc64 * 1e-3) / 1e9 / peak,
