@@ -33,6 +33,7 @@ struct EnsRep {
     const cpx<float> *tw[3];
     const float *g[3];
     double *qpart, *Qd, *partials;
+    float *acc;  // (A, B) concentration sums formed in the chain (h-in-pencil groups with phi_in_chain), or null
     float *Dh[kRedWidth], *wh[kRedWidth];  // FP32 history (the FP32-mixed context's)
     // Anderson loop state
     int phys[kRedWidth];  // logical history slot -> physical buffer
@@ -90,6 +91,13 @@ __global__ void __launch_bounds__(C3::NT, 1)
     a.Nd = (double)R.N;
     if (MODE == PLANE_INIT_W) {
         a.qout = R.q;
+    } else if (MODE == PLANE_G) {
+        // the h-in-pencil chain's plane (enqueue_chain_launches): g from the
+        // separable tables; ahead of a summing pencil, its partner slot to L2
+        a.gx = R.g[0];
+        a.gy = R.g[1];
+        a.gz = R.g[2];
+        if (R.acc && R.N - i < i + 1) a.pf = R.q + (long long)(R.N - i - 1) * 2 * R.M;
     } else {
         a.h = R.q;
         a.qout = R.q + (long long)i * 2 * R.M;
@@ -97,6 +105,57 @@ __global__ void __launch_bounds__(C3::NT, 1)
         a.hsel1 = i < R.NB ? 1 : 0;
     }
     plane3_body<C3, MODE>(a, blockIdx.x, R.mx);
+}
+
+// The h-in-pencil chain's x-pencils (the single context's
+// enqueue_chain_launches, same arguments): INIT_W (h from the fields, stored
+// as slot 1), H (store slot i+1), and, from the middle of the chain on when
+// the replica forms its concentration sums in the chain (R.acc), HA / HA_LAST
+// (add the slot's products with its stored partner slot N-i).
+template <int NX, int CW, int MODE>
+__global__ void __launch_bounds__(PencilCfg<float, NX, CW>::NT)
+    ens_pencil_x_kernel(EnsRep *__restrict__ reps, const int *__restrict__ members, int i)
+{
+    const EnsRep &R = reps[members[blockIdx.y]];
+    if (!R.active) return;
+    PencilArgs<float> a{};
+    a.spec = R.spec;
+    a.twx = R.tw[0];
+    a.gx = R.g[0];
+    a.gy = R.g[1];
+    a.gz = R.g[2];
+    a.ncol = R.my * R.mz;
+    a.KZ = R.mz;
+    a.w = R.w;
+    a.h = R.q;  // slot 1: the (hA, hB) pairs
+    a.M = R.M;
+    a.Nd = (double)R.N;
+    if (MODE == PENCIL_INIT_W) {
+        a.qout = R.q;
+    } else {
+        a.qout = R.q + (long long)i * 2 * R.M;  // slot i+1
+        a.hsel0 = i < R.NA ? 0 : 1;              // src/step.cc:53-57
+        a.hsel1 = i < R.NB ? 1 : 0;              // src/step.cc:60-64
+        if (MODE == PENCIL_HA || MODE == PENCIL_HA_LAST) {
+            const int p = R.N - i;  // partner slot
+            a.partner = p < i + 1 ? R.q + (long long)(p - 1) * 2 * R.M : nullptr;
+            a.acc = R.acc;
+            a.acc_init = i == (R.N - 1 + 1) / 2 ? 1 : 0;  // the first step with p <= i + 1
+            a.a_is_A = i + 1 <= R.NA;
+            a.b_is_A = p <= R.NA;
+        }
+    }
+    pencil_body<float, NX, CW, MODE>(a, blockIdx.x, 0);
+}
+
+// Q's per-plane partials from slot N of every member (plane_q_sums_kernel
+// per replica): grid (mx, members)
+__global__ void __launch_bounds__(256) ens_plane_q_sums_kernel(EnsRep *__restrict__ reps, const int *__restrict__ members)
+{
+    const EnsRep &R = reps[members[blockIdx.y]];
+    if (!R.active || (int)blockIdx.x >= R.mx) return;
+    plane_q_sums_body(reinterpret_cast<const float2 *>(R.q + (long long)(R.N - 1) * 2 * R.M),
+                      (long long)R.my * R.mz, R.qpart, blockIdx.x);
 }
 
 template <int NX, int CW>
@@ -132,16 +191,22 @@ __global__ void __launch_bounds__(256) ens_qfinal_kernel(EnsRep *__restrict__ re
     }
 }
 
-// phi, the residual Dh0 and its dot products: grid (max red_blocks, nrep)
-__global__ void __launch_bounds__(kRedThreads, 4) ens_conc_kernel(EnsRep *__restrict__ reps)
+// phi, the residual Dh0 and its dot products: grid (max red_blocks, nrep), or
+// (max red_blocks, group size) over `members`
+__global__ void __launch_bounds__(kRedThreads, 4) ens_conc_kernel(EnsRep *__restrict__ reps,
+                                                                  const int *__restrict__ members)
 {
-    const EnsRep &R = reps[blockIdx.y];
+    const EnsRep &R = reps[members ? members[blockIdx.y] : blockIdx.y];
     if (!R.active || (int)blockIdx.x >= R.red_blocks) return;
     const int nh = ens_nh(R.k);
     HistPtrs hist{};
     for (int m = 1; m <= nh; m++) hist.p[m - 1] = R.Dh[R.phys[m]];
-    concentrations_body<float>(R.q, R.M, R.N, R.NA, R.w, R.w + 2 * R.M, R.w + 3 * R.M, R.Qd, R.Dh[R.cur], nh, hist,
-                               R.partials, blockIdx.x, R.red_blocks);
+    if (R.acc)  // phi from the sums the chain formed (concentrations_acc_kernel)
+        concentrations_acc_body(R.acc, R.q, R.M, R.N, R.w + 2 * R.M, R.w + 3 * R.M, R.Qd, R.Dh[R.cur], nh, hist,
+                                R.partials, blockIdx.x, R.red_blocks);
+    else
+        concentrations_body<float>(R.q, R.M, R.N, R.NA, R.w, R.w + 2 * R.M, R.w + 3 * R.M, R.Qd, R.Dh[R.cur], nh,
+                                   hist, R.partials, blockIdx.x, R.red_blocks);
 }
 
 // One replica per block: the reduction of its dot products (as

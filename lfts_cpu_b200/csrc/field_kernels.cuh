@@ -57,15 +57,22 @@ static __global__ void q_finalize_kernel(const double *qpart, int n, long long M
 // Per-plane sums of chain 1's last propagator q_N (the first component of the
 // stored FP32 pairs), one CTA per x-plane in a fixed order: the partials
 // q_finalize_kernel reduces, for the chain that stores q in the x-pencil.
-static __global__ void __launch_bounds__(256) plane_q_sums_kernel(const float2 *__restrict__ qN, long long plane,
-                                                                  double *qpart)
+// (body: plane x of one field; the ensemble's batched launch calls it per replica)
+__device__ __forceinline__ void plane_q_sums_body(const float2 *__restrict__ qN, long long plane, double *qpart,
+                                                  const int x)
 {
     __shared__ double sh[32];
-    const float2 *p = qN + blockIdx.x * plane;
+    const float2 *p = qN + x * plane;
     double s = 0.0;
     for (long long i = threadIdx.x; i < plane; i += blockDim.x) s += (double)p[i].x;
     s = block_sum(s, sh);
-    if (threadIdx.x == 0) qpart[blockIdx.x] = s;
+    if (threadIdx.x == 0) qpart[x] = s;
+}
+
+static __global__ void __launch_bounds__(256) plane_q_sums_kernel(const float2 *__restrict__ qN, long long plane,
+                                                                  double *qpart)
+{
+    plane_q_sums_body(qN, plane, qpart, blockIdx.x);
 }
 
 template <typename T, int V>

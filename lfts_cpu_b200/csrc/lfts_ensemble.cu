@@ -6,12 +6,15 @@
 // Langevin step of every replica as one CUDA graph:
 //
 //   [Langevin update, all replicas] -> [begin] -> WHILE (any replica active) {
-//       per mesh group, on its own stream: INIT_W plane, N-1 x (x-pencil, plane)
+//       per mesh group, on its own stream: the contour chain in the group's
+//       tuned order (enqueue_group_chain)
 //       -> Q, concentrations + dots, reduction + least squares, w+ update,
 //       control (sets the WHILE condition) }
 //
 // so a step costs one graph launch and no host round trip.
 #include <cmath>
+#include <cstddef>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -118,6 +121,40 @@ bool ens_plane(int ny, int nz, int stages, PlaneSet *o)
     return false;
 }
 
+// the h-in-pencil chain's x-pencils (96-point lines, as a single context's)
+using PencilXFn = void (*)(EnsRep *, const int *, int);
+struct PencilXSet {
+    PencilXFn fn[kPencilModes];
+    PlaneFn plane_g;  // the chain's yz-plane kernel (PLANE_G, three stages)
+    int nt;
+    size_t smem;
+};
+
+template <int N, int CW>
+void fill_pencil_x(PencilXSet *o)
+{
+    using C = PencilCfg<float, N, CW>;
+    for (int m = 0; m < kPencilModes; m++) o->fn[m] = nullptr;
+    o->fn[PENCIL_INIT_W] = ens_pencil_x_kernel<N, CW, PENCIL_INIT_W>;
+    o->fn[PENCIL_H] = ens_pencil_x_kernel<N, CW, PENCIL_H>;
+    o->fn[PENCIL_H_LAST] = ens_pencil_x_kernel<N, CW, PENCIL_H_LAST>;
+    o->fn[PENCIL_HA] = ens_pencil_x_kernel<N, CW, PENCIL_HA>;
+    o->fn[PENCIL_HA_LAST] = ens_pencil_x_kernel<N, CW, PENCIL_HA_LAST>;
+    o->plane_g = ens_plane3_kernel<Plane3_96, PLANE_G>;
+    o->nt = C::NT;
+    o->smem = C::SMEM;
+}
+
+// cubic 96^3 replicas only (the plane kernel is the three-stage 96 x 96 one)
+bool ens_pencil_x(int nx, int ny, int nz, int cw, PencilXSet *o)
+{
+    if (nx != 96 || ny != 96 || nz != 96) return false;
+    if (cw == 8) { fill_pencil_x<96, 8>(o); return true; }
+    if (cw == 16) { fill_pencil_x<96, 16>(o); return true; }
+    if (cw == 32) { fill_pencil_x<96, 32>(o); return true; }
+    return false;
+}
+
 bool ens_pencil(int nx, int cw, PencilSet *o)
 {
 #define X(n)                                                \
@@ -134,10 +171,12 @@ bool ens_pencil(int nx, int cw, PencilSet *o)
 
 struct Group {
     int mx = 0, my = 0, mz = 0, cw = 0, stages = 2;
+    int xh = 0, phi = 0;  // h-in-pencil chain; concentration sums in it
     std::vector<int> members;
     int *d_members = nullptr;
     PlaneSet pl{};
     PencilSet pe{};
+    PencilXSet px{};
     cudaStream_t st = nullptr;
     cudaEvent_t join = nullptr;
 };
@@ -185,29 +224,57 @@ struct EnsDeviceGuard {
     }
 };
 
+// one contour chain of every member of group g, on g.st; returns the launches.
+// Two chain orders, as a single context's (enqueue_chain_launches):
+//   h in the plane: INIT_W plane, N-1 x (x-pencil with g, plane with h storing slot i+1)
+//   h in the pencil (96^3): INIT_W pencil, N-1 x (plane with g, pencil with h
+//     storing slot i+1 -- or, with the sums in the chain, adding the products
+//     with the stored partner slot from the middle on), then Q's plane partials
+long long enqueue_group_chain(lfts_ensemble *e, Group &g)
+{
+    const int nm = (int)g.members.size();
+    const dim3 pgrid(g.mx, nm);
+    const dim3 egrid((g.my * g.mz + g.cw - 1) / g.cw, nm);
+    long long n = 0;
+    if (g.xh) {
+        g.px.fn[PENCIL_INIT_W]<<<egrid, g.px.nt, g.px.smem, g.st>>>(e->d_reps, g.d_members, 0);
+        n++;
+        for (int i = 1; i < e->N; i++) {
+            g.px.plane_g<<<pgrid, g.pl.nt, g.pl.smem, g.st>>>(e->d_reps, g.d_members, i);
+            const int p = e->N - i;  // partner slot
+            const bool last = i + 1 == e->N;
+            const int mode = (!g.phi || p > i + 1) ? (last ? PENCIL_H_LAST : PENCIL_H)
+                                                   : (last ? PENCIL_HA_LAST : PENCIL_HA);
+            g.px.fn[mode]<<<egrid, g.px.nt, g.px.smem, g.st>>>(e->d_reps, g.d_members, i);
+            n += 2;
+        }
+        ens_plane_q_sums_kernel<<<pgrid, 256, 0, g.st>>>(e->d_reps, g.d_members);
+        return n + 1;
+    }
+    g.pl.fn[PLANE_INIT_W]<<<pgrid, g.pl.nt, g.pl.smem, g.st>>>(e->d_reps, g.d_members, 0);
+    n++;
+    for (int i = 1; i < e->N; i++) {
+        g.pe.fn<<<egrid, g.pe.nt, g.pe.smem, g.st>>>(e->d_reps, g.d_members);
+        g.pl.fn[i + 1 < e->N ? PLANE_STEP : PLANE_LAST]<<<pgrid, g.pl.nt, g.pl.smem, g.st>>>(e->d_reps, g.d_members,
+                                                                                           i);
+        n += 2;
+    }
+    return n;
+}
+
 // one iteration of every active replica, enqueued on e->s0 (being captured)
 int enqueue_body(lfts_ensemble *e, int maxIter, double tol, cudaGraphConditionalHandle loop)
 {
     EK(cudaEventRecord(e->fork, e->s0));
     for (Group &g : e->groups) {
         EK(cudaStreamWaitEvent(g.st, e->fork, 0));
-        const int nm = (int)g.members.size();
-        const dim3 pgrid(g.mx, nm);
-        const dim3 egrid((g.my * g.mz + g.cw - 1) / g.cw, nm);
-        g.pl.fn[PLANE_INIT_W]<<<pgrid, g.pl.nt, g.pl.smem, g.st>>>(e->d_reps, g.d_members, 0);
-        e->launches++;
-        for (int i = 1; i < e->N; i++) {
-            g.pe.fn<<<egrid, g.pe.nt, g.pe.smem, g.st>>>(e->d_reps, g.d_members);
-            g.pl.fn[i + 1 < e->N ? PLANE_STEP : PLANE_LAST]<<<pgrid, g.pl.nt, g.pl.smem, g.st>>>(e->d_reps,
-                                                                                               g.d_members, i);
-            e->launches += 2;
-        }
+        e->launches += enqueue_group_chain(e, g);
         EK(cudaGetLastError());
         EK(cudaEventRecord(g.join, g.st));
         EK(cudaStreamWaitEvent(e->s0, g.join, 0));
     }
     ens_qfinal_kernel<<<e->nrep, 256, 0, e->s0>>>(e->d_reps);
-    ens_conc_kernel<<<dim3(e->max_blocks, e->nrep), kRedThreads, 0, e->s0>>>(e->d_reps);
+    ens_conc_kernel<<<dim3(e->max_blocks, e->nrep), kRedThreads, 0, e->s0>>>(e->d_reps, nullptr);
     ens_reduce_solve_kernel<<<e->nrep, 256, 0, e->s0>>>(e->d_reps, tol, maxIter);
     ens_update_kernel<<<dim3(e->max_blocks, e->nrep), 256, 0, e->s0>>>(e->d_reps, e->d_lambda);
     ens_control_kernel<<<1, 256, 0, e->s0>>>(e->d_reps, e->nrep, loop, e->d_guard, e->guard_cap);
@@ -384,48 +451,92 @@ int ensure_graphs(lfts_ensemble *e, int maxIter, double tol)
 
 // ---- batched tile choice ---------------------------------------------------------
 // Each mesh group's tiles (x-pencil width 8/16/32; yz-plane stages 3 or 2 where
-// both exist) are picked by timing the group's batched contour chain, all its
-// replicas active, on its own stream -- batched, the best tiles differ from a
-// single context's (the plane launches run in several waves) -- once per
-// (mesh, group size, N) per process.  The choice is installed in every member
-// context too, so lfts_get_tiles on a replica's context, or lfts_set_tiles on
-// a single context, gives exactly the tiles the replica computes with.
+// both exist; at 96^3 also the h-in-pencil chain, with or without the
+// concentration sums in it) are picked by timing the group's batched contour
+// chain and concentration pass, all its replicas active, on its own stream --
+// batched, the best tiles differ from a single context's (the plane launches
+// run in several waves) -- once per (mesh, group size, N) per process.  The
+// choice is installed in every member context too, so lfts_get_tiles on a
+// replica's context, or lfts_set_tiles on a single context, gives exactly the
+// tiles the replica computes with.
+struct GroupTiles {
+    int cw, stages, xh, phi;
+};
 std::mutex g_ens_tune_mu;
-std::map<std::tuple<int, int, int, int, int>, std::pair<int, int>> g_ens_tuned;  // -> (cw, stages)
+std::map<std::tuple<int, int, int, int, int>, GroupTiles> g_ens_tuned;
 
-int set_group_tiles(Group &g, int cw, int stages)
+int set_group_tiles(Group &g, const GroupTiles &t)
 {
     PlaneSet pl{};
     PencilSet pe{};
-    if (!ens_plane(g.my, g.mz, stages, &pl) || !ens_pencil(g.mx, cw, &pe)) return LFTS_ERR_UNSUPPORTED;
+    PencilXSet px{};
+    if (!ens_plane(g.my, g.mz, t.stages, &pl) || !ens_pencil(g.mx, t.cw, &pe)) return LFTS_ERR_UNSUPPORTED;
+    if (t.phi && !t.xh) return LFTS_ERR_UNSUPPORTED;
+    if (t.xh && (t.stages != 3 || !ens_pencil_x(g.mx, g.my, g.mz, t.cw, &px))) return LFTS_ERR_UNSUPPORTED;
     for (int m = 0; m < 4; m++)
         EK(cudaFuncSetAttribute(pl.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
     EK(cudaFuncSetAttribute(pe.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pe.smem));
+    if (t.xh) {
+        EK(cudaFuncSetAttribute(px.plane_g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
+        for (int m = 0; m < kPencilModes; m++)
+            if (px.fn[m])
+                EK(cudaFuncSetAttribute(px.fn[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)px.smem));
+    }
     g.pl = pl;
     g.pe = pe;
-    g.cw = cw;
-    g.stages = stages;
+    g.px = px;
+    g.cw = t.cw;
+    g.stages = t.stages;
+    g.xh = t.xh;
+    g.phi = t.phi;
     return LFTS_OK;
 }
 
-void enqueue_group_chain(lfts_ensemble *e, Group &g)
+// the group's tiles into its member contexts, and each member's sum buffer
+// (allocated by the context when its tiles form the sums in the chain) into
+// its device descriptor
+int install_group_tiles(lfts_ensemble *e, const Group &g)
 {
-    const int nm = (int)g.members.size();
-    const dim3 pgrid(g.mx, nm);
-    const dim3 egrid((g.my * g.mz + g.cw - 1) / g.cw, nm);
-    g.pl.fn[PLANE_INIT_W]<<<pgrid, g.pl.nt, g.pl.smem, g.st>>>(e->d_reps, g.d_members, 0);
-    for (int i = 1; i < e->N; i++) {
-        g.pe.fn<<<egrid, g.pe.nt, g.pe.smem, g.st>>>(e->d_reps, g.d_members);
-        g.pl.fn[i + 1 < e->N ? PLANE_STEP : PLANE_LAST]<<<pgrid, g.pl.nt, g.pl.smem, g.st>>>(e->d_reps, g.d_members,
-                                                                                           i);
+    const lfts_tiles t{g.cw, g.stages, g.xh, 0, g.phi};
+    for (int r : g.members) {
+        int rc = lfts_set_tiles(e->rep[r], &t);
+        if (rc) return rc;
+        float *acc = g.phi ? static_cast<float *>(e->rep[r]->acc) : nullptr;
+        if (g.phi && !acc) return LFTS_ERR_NOMEM;
+        e->h_reps[r].acc = acc;
+        EK(cudaMemcpy(reinterpret_cast<char *>(e->d_reps + r) + offsetof(EnsRep, acc), &acc, sizeof(acc),
+                      cudaMemcpyHostToDevice));
     }
+    return LFTS_OK;
+}
+
+std::vector<GroupTiles> group_candidates(const Group &g)
+{
+    const char *fcw = std::getenv("LFTS_PENCIL_CW");
+    const char *fxh = std::getenv("LFTS_XH_CHAIN");
+    const char *fphi = std::getenv("LFTS_PHI_IN_CHAIN");
+    const int cw_forced = fcw ? std::atoi(fcw) : 0;
+    std::vector<GroupTiles> out;
+    PencilXSet px{};
+    for (int stages : {3, 2})
+        for (int cw : {8, 16, 32}) {
+            if (cw_forced > 0 && cw != cw_forced) continue;
+            for (int xh : {0, 1}) {
+                if (xh && (stages != 3 || !ens_pencil_x(g.mx, g.my, g.mz, cw, &px))) continue;
+                if (fxh && ((fxh[0] != '0') != (xh == 1))) continue;
+                for (int phi : {0, 1}) {
+                    if (phi && !xh) continue;
+                    if (fphi && xh && ((fphi[0] != '0') != (phi == 1))) continue;
+                    out.push_back({cw, stages, xh, phi});
+                }
+            }
+        }
+    return out;
 }
 
 int tune_groups(lfts_ensemble *e)
 {
     const char *off = std::getenv("LFTS_AUTOTUNE");
-    const char *fcw = std::getenv("LFTS_PENCIL_CW");
-    const int cw_forced = fcw ? std::atoi(fcw) : 0;
     // every replica active, so that the batched kernels do their work
     ens_begin_kernel<<<1, 256, 0, e->s0>>>(e->d_reps, e->nrep, e->d_step, 0, nullptr, 0, 0);
     EK(cudaStreamSynchronize(e->s0));
@@ -435,9 +546,21 @@ int tune_groups(lfts_ensemble *e)
     int rc = LFTS_OK;
     for (Group &g : e->groups) {
         const auto key = std::make_tuple(g.mx, g.my, g.mz, (int)g.members.size(), e->N);
-        std::pair<int, int> best{cw_forced > 0 ? cw_forced : 16, 2};
-        PlaneSet p3{};
-        if (ens_plane(g.my, g.mz, 3, &p3)) best.second = 3;
+        const std::vector<GroupTiles> cand = group_candidates(g);
+        if (cand.empty()) {
+            rc = LFTS_ERR_UNSUPPORTED;
+            break;
+        }
+        // without timing: 16 columns (or the forced width), three stages where
+        // they exist, h in the plane
+        const char *fcw = std::getenv("LFTS_PENCIL_CW");
+        const int cw_def = fcw && std::atoi(fcw) > 0 ? std::atoi(fcw) : 16;
+        GroupTiles best = cand.front();
+        for (const GroupTiles &t : cand)
+            if (t.cw == cw_def && !t.xh) {
+                best = t;
+                break;
+            }
         if (!(off && off[0] == '0')) {
             std::lock_guard<std::mutex> lk(g_ens_tune_mu);
             auto it = g_ens_tuned.find(key);
@@ -446,38 +569,44 @@ int tune_groups(lfts_ensemble *e)
             } else {
                 float best_ms = 0.f;
                 bool found = false;
-                for (int stages : {3, 2})
-                    for (int cw : {8, 16, 32}) {
-                        if (cw_forced > 0 && cw != cw_forced) continue;
-                        if (set_group_tiles(g, cw, stages) != LFTS_OK) continue;
-                        enqueue_group_chain(e, g);  // warm-up
-                        cudaEventRecord(e0, g.st);
-                        for (int r = 0; r < 3; r++) enqueue_group_chain(e, g);
-                        cudaEventRecord(e1, g.st);
-                        cudaError_t ce = cudaEventSynchronize(e1);
-                        if (ce == cudaSuccess) ce = cudaGetLastError();
-                        float ms = 0.f;
-                        if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
-                        if (ce != cudaSuccess) {
-                            lfts_internal_set_error(cudaGetErrorString(ce));
-                            rc = LFTS_ERR_CUDA;
-                            break;
-                        }
-                        if (!found || ms < best_ms) {
-                            best_ms = ms;
-                            best = {cw, stages};
-                            found = true;
-                        }
+                const dim3 cgrid(e->max_blocks, (unsigned)g.members.size());
+                for (const GroupTiles &t : cand) {
+                    if (set_group_tiles(g, t) != LFTS_OK) continue;
+                    if ((rc = install_group_tiles(e, g))) break;
+                    auto once = [&] {
+                        enqueue_group_chain(e, g);
+                        ens_conc_kernel<<<cgrid, kRedThreads, 0, g.st>>>(e->d_reps, g.d_members);
+                    };
+                    once();  // warm-up
+                    cudaEventRecord(e0, g.st);
+                    for (int r = 0; r < 3; r++) once();
+                    cudaEventRecord(e1, g.st);
+                    cudaError_t ce = cudaEventSynchronize(e1);
+                    if (ce == cudaSuccess) ce = cudaGetLastError();
+                    float ms = 0.f;
+                    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+                    if (ce != cudaSuccess) {
+                        lfts_internal_set_error(cudaGetErrorString(ce));
+                        rc = LFTS_ERR_CUDA;
+                        break;
                     }
+                    if (const char *v = std::getenv("LFTS_VERBOSE"))
+                        if (v[0] == '1')
+                            fprintf(stderr, "lfts: ensemble group %dx%dx%d (%d replicas) cw %d stages %d h_in_pencil %d "
+                                    "phi_in_chain %d: %.4f ms per chain + concentrations\n",
+                                    g.mx, g.my, g.mz, (int)g.members.size(), t.cw, t.stages, t.xh, t.phi, ms / 3.0f);
+                    if (!found || ms < best_ms) {
+                        best_ms = ms;
+                        best = t;
+                        found = true;
+                    }
+                }
                 if (rc) break;
                 if (found) g_ens_tuned[key] = best;
             }
         }
-        if ((rc = set_group_tiles(g, best.first, best.second))) break;
-        const lfts_tiles t{best.first, best.second, 0, 0};
-        for (int r : g.members)
-            if ((rc = lfts_set_tiles(e->rep[r], &t))) break;
-        if (rc) break;
+        if ((rc = set_group_tiles(g, best))) break;
+        if ((rc = install_group_tiles(e, g))) break;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -580,6 +709,7 @@ int lfts_ensemble_create(const lfts_params *params, const unsigned long long *se
         R.qpart = c->qpart;
         R.Qd = c->Qd;
         R.partials = c->partials;
+        R.acc = nullptr;  // set by the group's tiles (install_group_tiles)
         for (int i = 0; i < kRedWidth; i++) {
             R.Dh[i] = static_cast<float *>(c->Dh[i]);
             R.wh[i] = static_cast<float *>(c->wh[i]);

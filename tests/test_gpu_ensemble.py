@@ -100,8 +100,10 @@ def test_batched_configuration_shape(lfts):
     assert all(e.tuning(r) in (8, 16, 32) for r in range(32))
     for r, mm in enumerate(meshes):
         t = e.tiles(r)
-        assert t["h_in_pencil"] == 0 and t["two_streams"] == 0
+        assert t["two_streams"] == 0
         assert t["plane_stages"] in ((3, 2) if mm in (64, 96) else (2,))
+        assert t["h_in_pencil"] in ((0, 1) if mm == 96 else (0,))
+        assert t["phi_in_chain"] <= t["h_in_pencil"]
     for r, d in enumerate(reps):
         w = e.get_fields(r)
         M = int(np.prod(d["m"]))
@@ -135,3 +137,41 @@ def test_ensemble_rejects_bad_input(lfts):
     with pytest.raises(LftsError):
         ens.mix(max_iter=1)
     ens.close()
+
+
+@pytest.mark.parametrize("N,NA,phi", [(10, 4, 0), (11, 4, 1), (12, 11, 1)])
+def test_h_in_pencil_replicas_equal_single_contexts(lfts, N, NA, phi):
+    """96^3 replicas on the h-in-pencil chain (forced for this group, with and
+    without the concentration sums formed in the chain; odd N pairs the middle
+    slot with itself; NA = 11 of 12 switches h at the last step) against single contexts with the
+    same tiles: bitwise, over a mix and two Langevin steps."""
+    import os
+    reps = [dict(N=N, NA=NA, XbN=14.0 + r, C=50.0, dt=0.5, m=(96, 96, 96), L=(6.0, 6.0, 6.0), seed=300 + r)
+            for r in range(2)]
+    rng = np.random.default_rng(N)
+    fields = [rng.normal(0.0, 0.3, 2 * 96 ** 3) for _ in reps]
+    saved = {k: os.environ.get(k) for k in ("LFTS_XH_CHAIN", "LFTS_PHI_IN_CHAIN")}
+    os.environ["LFTS_XH_CHAIN"] = "1"
+    os.environ["LFTS_PHI_IN_CHAIN"] = str(phi)
+    try:
+        e = lfts.Ensemble(reps)
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    for r, w2 in enumerate(fields):
+        e.set_fields(r, w2)
+    k0, lnq0 = e.mix()
+    ks, lnq = e.run(2)
+    tiles = [e.tiles(r) for r in range(len(reps))]
+    w = [e.get_fields(r) for r in range(len(reps))]
+    e.close()
+    for r, d in enumerate(reps):
+        assert tiles[r]["h_in_pencil"] == 1 and tiles[r]["phi_in_chain"] == phi and tiles[r]["plane_stages"] == 3
+        sk0, slnq0, _, sks, slnq, sw = single_run(lfts, d, fields[r], 2, tiles[r])
+        assert k0[r] == sk0 and lnq0[r] == slnq0
+        assert list(ks[:, r]) == sks
+        assert lnq[r] == slnq
+        assert np.array_equal(w[r], sw)
