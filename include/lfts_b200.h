@@ -189,13 +189,17 @@ typedef struct lfts_tiles {
                           middle of the chain on (each new slot times its already stored partner,
                           FP32 sums; the later slots are then not stored) (1), or by a separate
                           pass over all N stored slots (0) */
+    int plane_split;   /* FP32-mixed 128 x 128 planes with h_in_pencil: CTAs per x-plane in the yz-plane
+                          kernel, 8 (the plane split over a thread-block cluster, its transposes through
+                          distributed shared memory; bitwise the same values) or 1; 0 reads as 1 */
 } lfts_tiles;
 /* lfts_create picks the tiles by timing the whole contour chain for every
  * valid combination on the context's own buffers and keeping the fastest,
  * once per precision and mesh in a process (the counterpart of the
  * reference's FFTW_PATIENT planning, src/step.cc:15-16).  Environment:
  * LFTS_AUTOTUNE=0 skips the timing (built-in choice); LFTS_PENCIL_CW=8|16|32,
- * LFTS_XH_CHAIN=0|1 and LFTS_ONE_STREAM=1 fix one choice each. */
+ * LFTS_XH_CHAIN=0|1, LFTS_PHI_IN_CHAIN=0|1, LFTS_PLANE_SPLIT=1|8 and
+ * LFTS_ONE_STREAM=1 fix one choice each. */
 int lfts_get_tiles(const lfts_ctx *ctx, lfts_tiles *out);
 /* Installs a tile choice (LFTS_ERR_ARG / LFTS_ERR_UNSUPPORTED for an
  * invalid one), e.g. to make a context compute exactly what an ensemble

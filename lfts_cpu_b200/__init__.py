@@ -231,8 +231,9 @@ class System:
         return t.as_dict()
 
     def set_tiles(self, pencil_cw: int, plane_stages: int, h_in_pencil: int = 0, two_streams: int = 0,
-                  phi_in_chain: int = 0) -> None:
-        t = Tiles(int(pencil_cw), int(plane_stages), int(h_in_pencil), int(two_streams), int(phi_in_chain))
+                  phi_in_chain: int = 0, plane_split: int = 1) -> None:
+        t = Tiles(int(pencil_cw), int(plane_stages), int(h_in_pencil), int(two_streams), int(phi_in_chain),
+                  int(plane_split))
         check(lib().lfts_set_tiles(self._h, C.byref(t)), "lfts_set_tiles")
 
     def profile_chain(self):

@@ -49,7 +49,7 @@ class Input(C.Structure):
 
 class Tiles(C.Structure):
     _fields_ = [("pencil_cw", C.c_int), ("plane_stages", C.c_int), ("h_in_pencil", C.c_int),
-                ("two_streams", C.c_int), ("phi_in_chain", C.c_int)]
+                ("two_streams", C.c_int), ("phi_in_chain", C.c_int), ("plane_split", C.c_int)]
 
     def as_dict(self):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}

@@ -68,6 +68,8 @@ struct lfts_ctx {
     PlaneKernels<float> pl32{};
     PencilKernels<float> pe32{};
     int plane_stages = 2;     // yz-plane transform stages per axis (3: fft_plane3.cuh)
+    int plane_split = 1;      // CTAs per x-plane of PLANE_G (8: the cluster kernel, fft_plane3c.cuh)
+    PlaneSplitKernel psplit{};
 
     bool fields_set = false;
     bool have_concs = false;

@@ -28,6 +28,14 @@ struct PencilKernels {
 bool plane_c_kernels(int ny, int nz, PlaneKernels<float> *out);
 // three-stage packed-chain plane kernels (fft_plane3.cuh), FP32: 64, 96, 128 square planes
 bool plane3_kernels(int ny, int nz, PlaneKernels<float> *out);
+// PLANE_G with each x-plane split over a thread-block cluster of cl CTAs
+// (fft_plane3c.cuh), FP32: 128 x 128 planes
+struct PlaneSplitKernel {
+    void (*fn)(PlaneArgs<float>);
+    int cl, nt;
+    size_t smem;
+};
+bool plane_split_kernel(int ny, int nz, PlaneSplitKernel *out);
 bool plane_kernels(int ny, int nz, PlaneKernels<double> *out);
 bool pencil_kernels(int nx, PencilKernels<double> *out);
 bool pencil_kernels(int nx, PencilKernels<float> *out);

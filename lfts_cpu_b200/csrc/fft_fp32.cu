@@ -1,6 +1,7 @@
 // FP32 instantiations of the contour-step FFT kernels (the FP32-mixed path).
 #include "fft_inst.cuh"
 #include "fft_plane3.cuh"
+#include "fft_plane3c.cuh"
 
 #define LFTS_PENCIL_CASE_float(a) \
     if (nx == a) { fill_pencil<float, a>(o); return true; }
@@ -43,5 +44,14 @@ bool plane3_kernels(int ny, int nz, PlaneKernels<float> *o)
     if (ny == 96) { fill_plane3<Plane3_96>(o); return true; }
     if (ny == 64) { fill_plane3<Plane3_64>(o); return true; }
     return false;
+}
+bool plane_split_kernel(int ny, int nz, PlaneSplitKernel *o)
+{
+    if (ny != 128 || nz != 128) return false;
+    o->fn = plane3_split_g_kernel<Plane3Split128>;
+    o->cl = Plane3Split128::CL;
+    o->nt = Plane3Split128::NT;
+    o->smem = Plane3Split128::SMEM;
+    return true;
 }
 }  // namespace lfts

@@ -223,6 +223,12 @@ void launch_pdl(lfts_ctx *c, K kernel, dim3 grid, int nt, size_t smem, const A &
 template <typename T>
 void launch_plane(lfts_ctx *c, int mode, const PlaneArgs<T> &a, int nchains, cudaStream_t st = nullptr)
 {
+    if constexpr (sizeof(T) == sizeof(float)) {
+        if (mode == PLANE_G && c->plane_split > 1) {
+            launch_pdl(c, c->psplit.fn, dim3(c->mx * c->psplit.cl), c->psplit.nt, c->psplit.smem, a, st);
+            return;
+        }
+    }
     const PlaneKernels<T> &pl = plane_of<T>(c);
     launch_pdl(c, pl.fn[mode], dim3(c->mx, c->packed ? 1 : nchains), pl.nt, pl.smem, a, st);
 }
@@ -479,9 +485,11 @@ void drop_chain_graph(lfts_ctx *c)
 int apply_tiles(lfts_ctx *c, const lfts_tiles &t)
 {
     if (t.pencil_cw != 8 && t.pencil_cw != 16 && t.pencil_cw != 32) return LFTS_ERR_ARG;
+    const int split = t.plane_split == 0 ? 1 : t.plane_split;
+    if (split != 1 && split != 8) return LFTS_ERR_ARG;
     if (c->prec == LFTS_FP64) {
         if (t.plane_stages != 2 || t.h_in_pencil != 0 || (t.two_streams != 0 && t.two_streams != 1) ||
-            t.phi_in_chain != 0)
+            t.phi_in_chain != 0 || split != 1)
             return LFTS_ERR_ARG;
         int rc = set_pencil<double>(c, t.pencil_cw);
         if (rc) return rc;
@@ -497,6 +505,13 @@ int apply_tiles(lfts_ctx *c, const lfts_tiles &t)
         if (!pencil_kernels(c->mx, t.pencil_cw, &pk)) return LFTS_ERR_UNSUPPORTED;
         if (t.h_in_pencil && !(pl.fn[PLANE_G] && pk.fn[PENCIL_H])) return LFTS_ERR_UNSUPPORTED;
         if (t.phi_in_chain && !(pk.fn[PENCIL_HA] && pk.fn[PENCIL_HA_LAST])) return LFTS_ERR_UNSUPPORTED;
+        PlaneSplitKernel ps{};
+        if (split > 1) {
+            // the cluster kernel replaces PLANE_G of the three-stage plane
+            if (!(t.h_in_pencil && t.plane_stages == 3 && plane_split_kernel(c->my, c->mz, &ps) && ps.cl == split))
+                return LFTS_ERR_UNSUPPORTED;
+            CK(cudaFuncSetAttribute(ps.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps.smem));
+        }
         if (t.phi_in_chain && !c->acc) {
             // the (A, B) concentration sums, FP32 pairs per mesh point
             cudaError_t e = cudaMalloc(&c->acc, sizeof(float) * 2 * (size_t)c->M);
@@ -512,6 +527,8 @@ int apply_tiles(lfts_ctx *c, const lfts_tiles &t)
         int rc = set_pencil<float>(c, t.pencil_cw);
         if (rc) return rc;
         c->pl32 = pl;
+        c->psplit = ps;
+        c->plane_split = split;
         c->plane_stages = t.plane_stages;
         c->xh_chain = t.h_in_pencil == 1;
         c->phi_in_chain = t.phi_in_chain == 1;
@@ -529,6 +546,7 @@ lfts_tiles current_tiles(const lfts_ctx *c)
     t.h_in_pencil = (!fp64 && c->xh_chain) ? 1 : 0;
     t.two_streams = (fp64 && c->two_streams) ? 1 : 0;
     t.phi_in_chain = (!fp64 && c->phi_in_chain) ? 1 : 0;
+    t.plane_split = fp64 ? 1 : c->plane_split;
     return t;
 }
 
@@ -542,13 +560,17 @@ std::vector<lfts_tiles> tile_candidates(const lfts_ctx *c)
     const char *fxh = std::getenv("LFTS_XH_CHAIN");
     const char *fone = std::getenv("LFTS_ONE_STREAM");
     const char *fphi = std::getenv("LFTS_PHI_IN_CHAIN");
+    const char *fsplit = std::getenv("LFTS_PLANE_SPLIT");
+    const int split_forced = fsplit ? std::atoi(fsplit) : 0;
+    PlaneSplitKernel ps{};
+    const bool has_split = c->prec != LFTS_FP64 && plane_split_kernel(c->my, c->mz, &ps);
     const int cw_forced = fcw ? std::atoi(fcw) : 0;
     for (int cw : {8, 16, 32}) {
         if (cw_forced > 0 && cw != cw_forced) continue;
         if (c->prec == LFTS_FP64) {
             for (int two : {1, 0}) {
                 if (fone && ((fone[0] == '1') == (two == 1))) continue;
-                out.push_back({cw, 2, 0, two, 0});
+                out.push_back({cw, 2, 0, two, 0, 1});
             }
             continue;
         }
@@ -565,7 +587,11 @@ std::vector<lfts_tiles> tile_candidates(const lfts_ctx *c)
                 for (int phi : {0, 1}) {
                     if (phi && (!xh || !hasa)) continue;
                     if (fphi && ((fphi[0] != '0') != (phi == 1))) continue;
-                    out.push_back({cw, st, xh, 0, phi});
+                    for (int split : {1, 8}) {
+                        if (split > 1 && !(xh && has_split && ps.cl == split)) continue;
+                        if (split_forced > 0 && split != split_forced) continue;
+                        out.push_back({cw, st, xh, 0, phi, split});
+                    }
                 }
             }
         }
@@ -581,7 +607,7 @@ lfts_tiles default_tiles(const lfts_ctx *c)
     const int cw = c->prec == LFTS_FP64 ? kDefaultCwFp64 : kDefaultCwFp32;
     for (const lfts_tiles &t : cand)
         if (t.pencil_cw == cw) return t;  // candidates come best-guess first
-    return cand.empty() ? lfts_tiles{cw, 2, 0, c->prec == LFTS_FP64 ? 1 : 0, 0} : cand.front();
+    return cand.empty() ? lfts_tiles{cw, 2, 0, c->prec == LFTS_FP64 ? 1 : 0, 0, 1} : cand.front();
 }
 
 // one calc_concs without the Anderson dot products: the chain, then the

@@ -497,7 +497,7 @@ int set_group_tiles(Group &g, const GroupTiles &t)
 // its device descriptor
 int install_group_tiles(lfts_ensemble *e, const Group &g)
 {
-    const lfts_tiles t{g.cw, g.stages, g.xh, 0, g.phi};
+    const lfts_tiles t{g.cw, g.stages, g.xh, 0, g.phi, 1};
     for (int r : g.members) {
         int rc = lfts_set_tiles(e->rep[r], &t);
         if (rc) return rc;

@@ -25,12 +25,13 @@ def lfts(native_lib):
 def candidates(precision, m):
     """Every tile combination, valid or not, for the context to accept or refuse."""
     out = []
-    for cw, st, xh, two, phi in itertools.product((8, 16, 32), (2, 3), (0, 1), (0, 1), (0, 1)):
-        if precision == 0 and (st != 2 or xh or phi):
+    for cw, st, xh, two, phi, split in itertools.product((8, 16, 32), (2, 3), (0, 1), (0, 1), (0, 1), (1, 8)):
+        if precision == 0 and (st != 2 or xh or phi or split != 1):
             continue
         if precision == 1 and (two or (phi and not xh)):
             continue
-        out.append(dict(pencil_cw=cw, plane_stages=st, h_in_pencil=xh, two_streams=two, phi_in_chain=phi))
+        out.append(dict(pencil_cw=cw, plane_stages=st, h_in_pencil=xh, two_streams=two, phi_in_chain=phi,
+                        plane_split=split))
     return out
 
 
@@ -40,6 +41,9 @@ def valid(precision, m, t):
     if t["plane_stages"] == 3 and m[1] not in (64, 96, 128):
         return False
     if t["h_in_pencil"] and not (t["plane_stages"] == 3 and m[0] in (96, 128) and m[1] in (96, 128)):
+        return False
+    # the cluster-split plane kernel: PLANE_G of 128 x 128 planes
+    if t["plane_split"] != 1 and not (t["h_in_pencil"] and m[1] == 128 and m[2] == 128):
         return False
     return True
 
@@ -89,7 +93,7 @@ def test_fp32_tiles_agree_within_tolerance(lfts, m, N, NA):
     for t, lnq, phi in res:
         assert abs(lnq - lnq64) < FP32_PHI_TOL * max(1.0, abs(lnq64)), t
         assert rel_err(phi, phi64) < FP32_PHI_TOL, t
-    # the pencil width alone changes no value
+    # the pencil width and the plane split change no value
     by_rest = {}
     for t, lnq, phi in res:
         key = (t["plane_stages"], t["h_in_pencil"], t["phi_in_chain"])
@@ -132,4 +136,34 @@ def test_phi_in_chain_matches_the_separate_pass(lfts, N, NA):
     assert rel_err(p1, p0) < FP32_PHI_TOL
     if q0 is not None:
         assert np.array_equal(q1, q0)
+    s.close()
+
+
+@pytest.mark.parametrize("N,NA,phi", [(2, 1, 0), (7, 3, 1), (8, 3, 0), (64, 25, 1)])
+def test_plane_split_is_bitwise_neutral(lfts, N, NA, phi):
+    """The yz-plane kernel with each 128 x 128 x-plane spread over a cluster of
+    8 CTAs (transposes through distributed shared memory) computes every value
+    the one-CTA-per-plane kernel computes: ln Q, phi and the propagators
+    bitwise equal."""
+    m = (128, 128, 128)
+    M = int(np.prod(m))
+    w2 = np.random.default_rng(N * 10 + phi).normal(0.0, 0.5, 2 * M)
+    s = lfts.System(N, NA, 16.0, 100.0, 0.5, m, (8.0, 8.0, 8.0), precision=1)
+    s.set_fields(w2)
+    out = []
+    for split in (1, 8):
+        s.set_tiles(16, 3, 1, 0, phi, split)
+        assert s.tiles()["plane_split"] == split
+        lnq = s.calc_concs()
+        out.append((lnq, s.get_fields()[2 * M:], s.propagators() if N <= 8 else None))
+    (lq0, p0, q0), (lq1, p1, q1) = out
+    assert lq1 == lq0
+    assert np.array_equal(p1, p0)
+    if q0 is not None:
+        assert np.array_equal(q1, q0)
+    # refused where the cluster kernel does not apply
+    with pytest.raises(lfts.LftsError):
+        s.set_tiles(16, 3, 0, 0, 0, 8)
+    with pytest.raises(lfts.LftsError):
+        s.set_tiles(16, 3, 1, 0, phi, 4)
     s.close()
