@@ -587,9 +587,11 @@ std::vector<lfts_tiles> tile_candidates(const lfts_ctx *c)
                 for (int phi : {0, 1}) {
                     if (phi && (!xh || !hasa)) continue;
                     if (fphi && ((fphi[0] != '0') != (phi == 1))) continue;
+                    // LFTS_PLANE_SPLIT applies where the cluster kernel does
+                    const bool can_split = xh && has_split && ps.cl == 8;
                     for (int split : {1, 8}) {
-                        if (split > 1 && !(xh && has_split && ps.cl == split)) continue;
-                        if (split_forced > 0 && split != split_forced) continue;
+                        if (split > 1 && !can_split) continue;
+                        if (split_forced > 0 && can_split && split != split_forced) continue;
                         out.push_back({cw, st, xh, 0, phi, split});
                     }
                 }
