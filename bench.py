@@ -595,6 +595,21 @@ def main(argv=None):
     part_chain, part_conc, part_upd = fp32_sys.profile_iteration(5)
     tiles32 = fp32_sys.tiles()
     ms_calc = time_calc_concs(fp32_sys, torch, device)
+    # the yz-plane kernel split over a thread-block cluster (tile plane_split)
+    # against the tuned choice: chain of one calc_concs, CUDA events
+    split_alt = None
+    alt = dict(tiles32, plane_split=8 if tiles32.get("plane_split", 1) == 1 else 1)
+    try:
+        fp32_sys.set_tiles(**alt)
+        ms_alt = min(fp32_sys.profile_iteration(3)[0] for _ in range(2))
+        fp32_sys.set_tiles(**tiles32)
+        ms_tuned = min(fp32_sys.profile_iteration(3)[0] for _ in range(2))
+        split_alt = {"tuned_plane_split": tiles32["plane_split"],
+                     "chain_ms": {str(tiles32["plane_split"]): ms_tuned, str(alt["plane_split"]): ms_alt},
+                     "note": "contour chain of one calc_concs with one CTA per 128x128 x-plane (1) or the plane "
+                             "spread over an 8-CTA cluster (8); results bitwise equal"}
+    except lfts.LftsError:
+        fp32_sys.set_tiles(**tiles32)
     # the contour step of a chain that stores every slot (the tuned chain may
     # form the concentration sums in its second half instead)
     ch_storing = None
@@ -708,6 +723,7 @@ def main(argv=None):
             "hbm_gbs_algorithmic_step": step_alg / (ms32 * 1e-3) / 1e9,
             "step_split": split_info,
             "tiles": tiles32,
+            "plane_split_alternative": split_alt,
             "fp64": {"value": world * 1e3 / ms64, "ms_per_step": ms64, "mean_anderson_K": K64,
                      "e2e": {"value": world * 1e3 / e2e64, "unit": "steps/s",
                              "h2d_bytes_per_step": fp64["h2d_bytes_per_step"],
