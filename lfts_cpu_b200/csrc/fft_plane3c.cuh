@@ -35,6 +35,7 @@ namespace lfts {
 
 template <typename C, int CL_>
 struct Plane3Split {
+    using Cfg = C;
     static constexpr int CL = CL_;
     static constexpr int NT = C::NT / CL;        // threads per CTA
     static constexpr int KZB = C::NZ / CL;       // S1 columns per CTA
@@ -79,7 +80,7 @@ __device__ __forceinline__ uint32_t cluster_rank()
 template <typename S>
 __global__ void __launch_bounds__(S::NT, 8) __cluster_dims__(S::CL, 1, 1) plane3_split_g_kernel(PlaneArgs<float> a)
 {
-    using C = Plane3_128;
+    using C = typename S::Cfg;
     constexpr int NY = C::NY, NZ = C::NZ, Y1 = C::Y1, Y2 = C::Y2, Z1 = C::Z1, Z2 = C::Z2, KP = C::KP;
     constexpr int KZB = S::KZB, K1B = S::K1B;
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -3,7 +3,8 @@ mix: a WHILE node around the contour chain, the concentrations with the
 residual dot products, the least squares on one warp, the w+ update) against
 the host-driven loop (the default; LFTS_DEVICE_MIX=1 selects the device loop): the same Anderson counts and the same
 fields bit for bit, over an initial mix and Langevin steps, both precisions,
-both FP32 chain orders."""
+both FP32 chain orders, the yz-plane kernel of 128 x 128 planes per CTA and
+split over a cluster."""
 import os
 
 import numpy as np
@@ -41,6 +42,8 @@ def make(lfts, host_loop, N, NA, m, precision, tiles=None):
     (1, (128, 128, 128), 8, 3, dict(pencil_cw=16, plane_stages=3, h_in_pencil=1, two_streams=0)),
     (1, (128, 128, 128), 8, 5, dict(pencil_cw=16, plane_stages=3, h_in_pencil=0, two_streams=0)),
     (1, (128, 128, 128), 7, 3, dict(pencil_cw=16, plane_stages=3, h_in_pencil=1, two_streams=0, phi_in_chain=1)),
+    (1, (128, 128, 128), 7, 3, dict(pencil_cw=16, plane_stages=3, h_in_pencil=1, two_streams=0, phi_in_chain=1,
+                                    plane_split=8)),
 ])
 def test_device_loop_equals_host_loop(lfts, precision, m, N, NA, tiles):
     M = int(np.prod(m))
