@@ -138,3 +138,34 @@ def test_ensemble_create_rejects_bad_replicas_before_any_device_call(native_lib,
     with pytest.raises(LftsError) as e:
         Ensemble(reps)
     assert e.value.status == status
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """The ctypes mirrors of the header's structs (lfts_params, lfts_input,
+    lfts_tiles) have the C compiler's size and field offsets, field by field."""
+    import ctypes
+    import shutil
+    import subprocess
+
+    from lfts_cpu_b200.capi import Input, Params, Tiles
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    structs = {"lfts_params": Params, "lfts_input": Input, "lfts_tiles": Tiles}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "lfts_b200.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in structs.items():
+        assert got[(cname, "sizeof")] == ctypes.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
