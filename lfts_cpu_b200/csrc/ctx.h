@@ -69,6 +69,7 @@ struct lfts_ctx {
     PencilKernels<float> pe32{};
     int plane_stages = 2;     // yz-plane transform stages per axis (3: fft_plane3.cuh)
     int plane_split = 1;      // CTAs per x-plane of PLANE_G (8: the cluster kernel, fft_plane3c.cuh)
+    int pf_ctas = 0;          // PLANE_G ahead of a summing pencil: prefetching CTAs past the planes
     PlaneSplitKernel psplit{};
 
     bool fields_set = false;

@@ -65,6 +65,7 @@ struct PlaneArgs {
     double Nd;            // N as a double (h = exp(-w/N))
     const T *gx, *gy, *gz;  // PLANE_G: separable Boltzmann weight, 1/M folded into gz
     const T *pf;          // PLANE_G: (chain 1, chain 2) slot that the next x-pencil reads, pulled into L2
+    int pf_ctas;          // PLANE_G with pf: CTAs past the planes that pull pf into L2 (0: each plane CTA its plane)
 };
 
 template <typename T, int NY, int NZ>

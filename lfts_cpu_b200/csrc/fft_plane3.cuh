@@ -295,7 +295,7 @@ __device__ __forceinline__ void plane3_body(const PlaneArgs<float> &a, const int
     // The summing x-pencil after this launch reads a stored slot written many
     // steps earlier, long gone from L2; this plane's share of it (plane x, one
     // float pair per point) is fetched into L2 while the transforms run.
-    if (MODE == PLANE_G && a.pf) {
+    if (MODE == PLANE_G && a.pf && a.pf_ctas == 0) {
         const char *base = reinterpret_cast<const char *>(a.pf + 2 * plane_off);
         constexpr int BYTES = 2 * C::NY * C::NZ * (int)sizeof(float);
         for (int o = 128 * threadIdx.x; o < BYTES; o += 128 * C::NT) prefetch_l2(base + o);
@@ -336,9 +336,33 @@ __device__ __forceinline__ void plane3_body(const PlaneArgs<float> &a, const int
     p3_s1_fwd<C>(P, Sg);
 }
 
+// A PLANE_G launch ahead of a summing x-pencil can carry pf_ctas CTAs past
+// the mx planes: they run on SMs the planes leave idle (128 planes, 148 SMs)
+// and pull the whole partner slot into L2 there, instead of each plane CTA
+// issuing its own plane's share between its transforms.
+template <typename C>
+__device__ __forceinline__ void p3_prefetch_tail(const PlaneArgs<float> &a, const int j, const int nj, const int mx)
+{
+    const char *base = reinterpret_cast<const char *>(a.pf);
+    const long long bytes = 2LL * mx * C::NY * C::NZ * (long long)sizeof(float);
+    const long long per = (bytes / nj + 127) / 128 * 128;
+    const long long lo = (long long)j * per;
+    const long long hi = lo + per < bytes ? lo + per : bytes;
+    for (long long o = lo + 128LL * threadIdx.x; o < hi; o += 128LL * C::NT) prefetch_l2(base + o);
+}
+
 template <typename C, int MODE>
 __global__ void __launch_bounds__(C::NT, 1) plane3_kernel(PlaneArgs<float> a)
 {
+    if (MODE == PLANE_G && a.pf_ctas > 0) {
+        const int mx = (int)gridDim.x - a.pf_ctas;
+        if ((int)blockIdx.x >= mx) {
+            if (a.pf) p3_prefetch_tail<C>(a, (int)blockIdx.x - mx, a.pf_ctas, mx);
+            return;
+        }
+        plane3_body<C, MODE>(a, blockIdx.x, mx);
+        return;
+    }
     plane3_body<C, MODE>(a, blockIdx.x, gridDim.x);
 }
 

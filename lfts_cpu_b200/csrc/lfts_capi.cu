@@ -230,7 +230,8 @@ void launch_plane(lfts_ctx *c, int mode, const PlaneArgs<T> &a, int nchains, cud
         }
     }
     const PlaneKernels<T> &pl = plane_of<T>(c);
-    launch_pdl(c, pl.fn[mode], dim3(c->mx, c->packed ? 1 : nchains), pl.nt, pl.smem, a, st);
+    const int extra = mode == PLANE_G ? a.pf_ctas : 0;
+    launch_pdl(c, pl.fn[mode], dim3(c->mx + extra, c->packed ? 1 : nchains), pl.nt, pl.smem, a, st);
 }
 
 template <typename T>
@@ -328,7 +329,10 @@ void enqueue_chain_launches(lfts_ctx *c)
             bool first_acc = true;
             for (int i = 1; i < c->N; i++) {
                 PlaneArgs<T> ag = a;
-                if (acc && c->N - i < i + 1) ag.pf = q + (long long)(c->N - i - 1) * 2 * M;  // the partner slot
+                if (acc && c->N - i < i + 1) {
+                    ag.pf = q + (long long)(c->N - i - 1) * 2 * M;  // the partner slot
+                    if (c->plane_split == 1) ag.pf_ctas = c->pf_ctas;
+                }
                 launch_plane<T>(c, PLANE_G, ag, 2);
                 PencilArgs<T> ph = pa;
                 ph.qout = q + (long long)i * 2 * M;  // slot i+1
@@ -1397,6 +1401,10 @@ int lfts_create(const lfts_params *p, int precision, int device, lfts_ctx **out)
     if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->sms = prop.multiProcessorCount;
     c->red_blocks = c->sms * 4;
     if (const char *e = getenv("LFTS_NO_PDL")) c->use_pdl = !(e[0] == '1');
+    // SMs the one-CTA-per-plane PLANE_G leaves idle take its L2 prefetch of the
+    // partner slot (LFTS_PREFETCH_CTAS=0: the plane CTAs issue it themselves)
+    c->pf_ctas = c->sms > c->mx ? std::min(c->sms - c->mx, 64) : 0;
+    if (const char *e = getenv("LFTS_PREFETCH_CTAS")) c->pf_ctas = std::max(0, std::min(std::atoi(e), c->pf_ctas));
     if (const char *e = getenv("LFTS_ONE_STREAM")) c->two_streams = !(e[0] == '1');
     if (const char *e = getenv("LFTS_NO_GRAPH")) c->use_graph = !(e[0] == '1');
     if (const char *e = getenv("LFTS_DEVICE_MIX")) c->mix_on_device = e[0] == '1';
