@@ -1402,8 +1402,10 @@ int lfts_create(const lfts_params *p, int precision, int device, lfts_ctx **out)
     c->red_blocks = c->sms * 4;
     if (const char *e = getenv("LFTS_NO_PDL")) c->use_pdl = !(e[0] == '1');
     // SMs the one-CTA-per-plane PLANE_G leaves idle take its L2 prefetch of the
-    // partner slot (LFTS_PREFETCH_CTAS=0: the plane CTAs issue it themselves)
-    c->pf_ctas = c->sms > c->mx ? std::min(c->sms - c->mx, 64) : 0;
+    // partner slot (LFTS_PREFETCH_CTAS=0: the plane CTAs issue it themselves).
+    // Only for 128 x 128 planes, whose CTA fills an SM's shared memory: at 96 x 96
+    // two plane CTAs share an SM and the extra CTAs measured slower
+    c->pf_ctas = (c->my == 128 && c->mz == 128 && c->sms > c->mx) ? std::min(c->sms - c->mx, 64) : 0;
     if (const char *e = getenv("LFTS_PREFETCH_CTAS")) c->pf_ctas = std::max(0, std::min(std::atoi(e), c->pf_ctas));
     if (const char *e = getenv("LFTS_ONE_STREAM")) c->two_streams = !(e[0] == '1');
     if (const char *e = getenv("LFTS_NO_GRAPH")) c->use_graph = !(e[0] == '1');
