@@ -298,16 +298,18 @@ static __global__ void __launch_bounds__(kRedThreads, 4) concentrations_kernel(
     concentrations_body<T>(q, M, N, NA, w, phim, phip, Qd, Dh0, nh, hist, partials, blockIdx.x, gridDim.x);
 }
 
-// out[m] = sum over blocks of partials[b][m], m < width, fixed order
+// out[m] = sum over blocks of partials[b][m], fixed order; block m < width
+// reduces column m (launch width blocks of 256 threads: every column's sum
+// is formed in the same order as by one block looping over the columns)
 static __global__ void reduce_partials_kernel(const double *partials, int nblocks, int width, double *out)
 {
     __shared__ double sh[32];
-    for (int m = 0; m < width; m++) {
-        double s = 0.0;
-        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += partials[(long long)b * kRedWidth + m];
-        s = block_sum(s, sh);
-        if (threadIdx.x == 0) out[m] = s;
-    }
+    const int m = blockIdx.x;
+    if (m >= width) return;
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += partials[(long long)b * kRedWidth + m];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) out[m] = s;
 }
 
 // w+ update of one Anderson iteration (src/anderson.cc:57-79) and the copy

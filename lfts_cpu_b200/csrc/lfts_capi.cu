@@ -419,7 +419,7 @@ void enqueue_concs(lfts_ctx *c, void *Dh0, int nh, const HistPtrs &hist)
             static_cast<T *>(Dh0), nh, hist, c->partials);
     c->launches++;
     if (Dh0) {
-        reduce_partials_kernel<<<1, 256, 0, c->st>>>(c->partials, c->red_blocks, nh + 1, c->red);
+        reduce_partials_kernel<<<nh + 1, 256, 0, c->st>>>(c->partials, c->red_blocks, nh + 1, c->red);
         c->launches++;
     }
 }
@@ -1644,7 +1644,7 @@ int lfts_get_H(lfts_ctx *c, double *H)
     int rc = calc_concs_sync(c, &lnQ);
     if (rc) return rc;
     h_sums_kernel<<<stream_grid(c), kRedThreads, 0, c->st>>>(c->w, c->M, c->partials);
-    reduce_partials_kernel<<<1, 256, 0, c->st>>>(c->partials, c->red_blocks, 2, c->red);
+    reduce_partials_kernel<<<2, 256, 0, c->st>>>(c->partials, c->red_blocks, 2, c->red);
     c->launches += 2;
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(c->red_host, c->red, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
@@ -1743,7 +1743,7 @@ int lfts_backward(lfts_ctx *c, int ckpt_every, double *dH_dL, double *dH_dXbN, d
         dH_dL[d] = -(kTwoPi * kTwoPi * S[d] / (3.0 * N * L * L * L)) / ((double)M * Q);
     }
     h_sums_kernel<<<stream_grid(c), kRedThreads, 0, c->st>>>(c->w, M, c->partials);
-    reduce_partials_kernel<<<1, 256, 0, c->st>>>(c->partials, c->red_blocks, 2, c->red);
+    reduce_partials_kernel<<<2, 256, 0, c->st>>>(c->partials, c->red_blocks, 2, c->red);
     c->launches += 2;
     CK(cudaMemcpyAsync(c->red_host, c->red, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -1799,7 +1799,7 @@ int lfts_profile_iteration(lfts_ctx *c, int reps, double *ms_chain, double *ms_c
             concentrations_kernel<float><<<stream_grid(c), kRedThreads, 0, c->st>>>(
                 static_cast<const float *>(c->q), M, c->N, c->NA, c->w, c->w + 2 * M, c->w + 3 * M, c->Qd,
                 static_cast<float *>(c->Dh[c->cur]), kMaxHist, Dhp, c->partials);
-        reduce_partials_kernel<<<1, 256, 0, c->st>>>(c->partials, c->red_blocks, kRedWidth, c->red);
+        reduce_partials_kernel<<<kRedWidth, 256, 0, c->st>>>(c->partials, c->red_blocks, kRedWidth, c->red);
     }
     CK(cudaEventRecord(ev[2], c->st));
     for (int r = 0; r < reps; r++) {
