@@ -163,6 +163,9 @@ int upload_tables(lfts_ctx *c, void **tw, void **gt)
 }
 
 inline dim3 stream_grid(const lfts_ctx *c) { return dim3(c->red_blocks); }
+// element-wise passes with no cross-block reduction (the Anderson w+ update):
+// a full wave of 256-thread CTAs, so more loads are in flight per SM
+inline dim3 update_grid(const lfts_ctx *c) { return dim3(c->sms * 8); }
 
 // ---- contour chain ----------------------------------------------------------
 template <typename T>
@@ -850,11 +853,11 @@ int anderson_mix_host(lfts_ctx *c, int maxIter, double errTol, int *k_out)
             }
         }
         if (c->prec == LFTS_FP64)
-            anderson_update_kernel<double><<<stream_grid(c), 256, 0, c->st>>>(
+            anderson_update_kernel<double><<<update_grid(c), 256, 0, c->st>>>(
                 c->w + M, static_cast<double *>(c->wh[c->cur]), static_cast<const double *>(Dh0), M, lambda, nh,
                 simple, Dhp, whp, C);
         else
-            anderson_update_kernel<float><<<stream_grid(c), 256, 0, c->st>>>(
+            anderson_update_kernel<float><<<update_grid(c), 256, 0, c->st>>>(
                 c->w + M, static_cast<float *>(c->wh[c->cur]), static_cast<const float *>(Dh0), M, lambda, nh,
                 simple, Dhp, whp, C);
         c->launches++;
@@ -1804,11 +1807,11 @@ int lfts_profile_iteration(lfts_ctx *c, int reps, double *ms_chain, double *ms_c
     CK(cudaEventRecord(ev[2], c->st));
     for (int r = 0; r < reps; r++) {
         if (c->prec == LFTS_FP64)
-            anderson_update_kernel<double><<<stream_grid(c), 256, 0, c->st>>>(
+            anderson_update_kernel<double><<<update_grid(c), 256, 0, c->st>>>(
                 c->w + M, static_cast<double *>(c->wh[c->cur]), static_cast<const double *>(c->Dh[c->cur]), M, 0.0,
                 kMaxHist, 0, Dhp, whp, zero);
         else
-            anderson_update_kernel<float><<<stream_grid(c), 256, 0, c->st>>>(
+            anderson_update_kernel<float><<<update_grid(c), 256, 0, c->st>>>(
                 c->w + M, static_cast<float *>(c->wh[c->cur]), static_cast<const float *>(c->Dh[c->cur]), M, 0.0,
                 kMaxHist, 0, Dhp, whp, zero);
     }
