@@ -163,8 +163,9 @@ int upload_tables(lfts_ctx *c, void **tw, void **gt)
 }
 
 inline dim3 stream_grid(const lfts_ctx *c) { return dim3(c->red_blocks); }
-// element-wise passes with no cross-block reduction (the Anderson w+ update):
-// a full wave of 256-thread CTAs, so more loads are in flight per SM
+// element-wise passes with no cross-block reduction (the Anderson w+ update,
+// the Langevin update): a full wave of 256-thread CTAs, so more loads are in
+// flight per SM
 inline dim3 update_grid(const lfts_ctx *c) { return dim3(c->sms * 8); }
 
 // ---- contour chain ----------------------------------------------------------
@@ -934,7 +935,7 @@ int capture_mix_graph(lfts_ctx *c, cudaGraph_t *g_out)
         mix_conc_kernel<T><<<stream_grid(c), kRedThreads, 0, c->st>>>(S, static_cast<const T *>(c->q), c->N, c->NA,
                                                                         c->Qd);
     mix_solve_kernel<<<1, 256, 0, c->st>>>(S);
-    mix_update_kernel<T><<<stream_grid(c), 256, 0, c->st>>>(S);
+    mix_update_kernel<T><<<update_grid(c), 256, 0, c->st>>>(S);
     mix_control_kernel<<<1, 32, 0, c->st>>>(S, loop);
     c->mix_body_kernels = c->launches - launches0 + 4;
     c->launches = launches0;
@@ -1535,7 +1536,7 @@ static int langevin_device(lfts_ctx *c, const double *eta_new_dev)
     const int nb = 1 - c->eta_prev;
     if (eta_new_dev != c->eta[nb])
         CK(cudaMemcpyAsync(c->eta[nb], eta_new_dev, sizeof(double) * c->M, cudaMemcpyDeviceToDevice, c->st));
-    langevin_kernel<<<stream_grid(c), 256, 0, c->st>>>(c->w, c->M, c->eta[c->eta_prev], c->eta[nb], c->p.XbN,
+    langevin_kernel<<<update_grid(c), 256, 0, c->st>>>(c->w, c->M, c->eta[c->eta_prev], c->eta[nb], c->p.XbN,
                                                        c->p.dt);
     c->launches++;
     CK(cudaGetLastError());
